@@ -1,0 +1,387 @@
+"""Benchmark of the LSD radix-sort hot path on B200.
+
+Workload (one "step"): a stable ascending LSD sort of 2^28 (268,435,456) uint32 keys drawn
+uniform over [0, 2^32) from seeded PCG32 streams -- the plain-sort-at-scale configuration
+the headline metric is quoted on.  Other dtypes/configs are parity-test cases.
+
+Arms
+  default (ours)   value: device-resident sorts through the C ABI (*_dev), CUDA events
+                   around each step on the context's stream, K steps over distinct copies
+                   of the input (inputs 1 GiB each > L2, restored between steps outside the
+                   events); e2e: the host-array C ABI call (H2D from pinned memory, sort,
+                   D2H into the same array) timed around each synchronous call.
+  --impl reference the CPU restatement of the reference's SortRadixPar (oracle, all host
+                   threads) on a bounded sample of the same keys per step.
+
+Multi-GPU (torchrun): the plain sort does not shard (each digit pass is a global
+permutation), so N ranks run N independent replicas ("replicas only", weak scaling);
+value = keys sorted by all ranks / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Gkeys/s & % HBM roofline (256M u32); batched/served vs plain, p50/p99, 1 B200"
+UNIT = "Gkeys/s"
+N_DEFAULT = 1 << 28
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--dtype", default="u32", choices=["u32", "i32", "f32", "u64", "i64", "f64"])
+    ap.add_argument("--slots", type=int, default=4, help="distinct input copies cycled through")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps (capped at 20)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.lines = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _in_order(a: np.ndarray) -> bool:
+    """Ascending in the library's key order (signed by value; floats by the sign-flip order)."""
+    u = a.view(np.uint32 if a.dtype.itemsize == 4 else np.uint64)
+    top = u.dtype.type(1) << u.dtype.type(8 * a.dtype.itemsize - 1)
+    if a.dtype.kind == "i":
+        u = u ^ top
+    elif a.dtype.kind == "f":
+        u = np.where((u & top) != 0, ~u, u ^ top)
+    return bool(np.all(u[1:] >= u[:-1]))
+
+
+def gen_keys(dtype: str, n: int, seed: int = 1) -> np.ndarray:
+    from hpcsharp_b200 import datagen
+
+    return datagen.by_name(dtype, n, seed)
+
+
+def read_traffic(dtype: str):
+    """DRAM bytes per onesweep launch from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", f"onesweep_pass_{dtype}_256M.txt")
+    try:
+        for line in open(p):
+            if line.startswith("dram_bytes_per_launch="):
+                return float(line.split("=", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------------------
+def cpu_baseline(dtype: str, n: int, budget_s: float = 15.0):
+    """The oracle's SortRadixPar restatement on the host cores, on a bounded sample."""
+    import oracle
+
+    oracle.build()
+    th = oracle.hardware_threads()
+    sample = min(n, 1 << 24)
+    a = gen_keys(dtype, sample, seed=7)
+    b = a.copy()
+    t0 = time.perf_counter()
+    oracle.sort_radix_par(b, threads=th)
+    dt = time.perf_counter() - t0
+    # grow the sample while the projected time for 3 repetitions stays inside the budget
+    while sample * 2 <= n and dt * 2 * 3 < budget_s:
+        sample *= 2
+        a = gen_keys(dtype, sample, seed=7)
+        b = a.copy()
+        t0 = time.perf_counter()
+        oracle.sort_radix_par(b, threads=th)
+        dt = time.perf_counter() - t0
+    times = []
+    for _ in range(3):
+        b = a.copy()
+        t0 = time.perf_counter()
+        oracle.sort_radix_par(b, threads=th)
+        times.append(time.perf_counter() - t0)
+    best = min(times)
+    return {"value": round(sample / best / 1e9, 4), "unit": UNIT, "cores": th, "kind": "port",
+            "sample": f"{sample} {dtype} keys (same generator), SortRadixPar C++ restatement, best of 3"}
+
+
+def run_reference(args, rank: int, world: int):
+    """--impl reference: the reference's SortRadixPar (C++ restatement; the C# reference
+    needs .NET, absent here) on the host cores; rank 0 only."""
+    if rank != 0:
+        return
+    import oracle
+
+    oracle.build()
+    th = oracle.hardware_threads()
+    n = args.n
+    sample = min(n, 1 << 26)
+    a = gen_keys(args.dtype, sample, seed=1)
+    # size the per-step sample so the whole run stays within ~2 minutes
+    t0 = time.perf_counter()
+    b = a.copy()
+    oracle.sort_radix_par(b, threads=th)
+    one = time.perf_counter() - t0
+    budget = 120.0 / max(1, args.steps + args.warmup)
+    while one > budget and sample > (1 << 20):
+        sample //= 2
+        one /= 2
+    a = a[:sample].copy()
+    for _ in range(args.warmup):
+        b = a.copy()
+        oracle.sort_radix_par(b, threads=th)
+    tot = 0.0
+    for _ in range(args.steps):
+        b = a.copy()
+        t0 = time.perf_counter()
+        oracle.sort_radix_par(b, threads=th)
+        tot += time.perf_counter() - t0
+    rate = sample * args.steps / tot / 1e9
+    line = {
+        "metric": METRIC, "value": round(rate, 4), "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tot / args.steps * 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.dtype,
+        "data": "synthetic (seeded PCG32 uniform)",
+        "config": {"workload": f"LSD radix sort, {n} {args.dtype} keys uniform; per step a {sample}-key sample",
+                   "n": n, "sample": sample, "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": round(rate, 4), "unit": UNIT, "cores": th, "kind": "port",
+                         "sample": f"{sample} keys per step; C++ restatement of SortRadixPar "
+                                   f"(RadixSortLsdParallel.cs:145-232), {th} threads"},
+        "e2e": {"value": round(rate, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+
+    from hpcsharp_b200 import native
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+
+    n, dtype = args.n, args.dtype
+    w = np.dtype(native.NP_OF[dtype]).itemsize
+    P = w
+    host = gen_keys(dtype, n, seed=1 + rank)
+    tview = {4: torch.int32, 8: torch.int64}[w]
+    src = torch.from_numpy(host.view({4: np.int32, 8: np.int64}[w])).to(f"cuda:{dev}")
+    slots = [src.clone() for _ in range(max(1, args.slots))]
+    ctx = native.Context(dev)
+    s = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{dev}")
+
+    def step(i):
+        ctx.sort_dev(slots[i % len(slots)], dtype=dtype)
+
+    def restore(i):
+        with torch.cuda.stream(s):
+            slots[i % len(slots)].copy_(src)
+
+    # warm-up
+    for i in range(args.warmup):
+        step(i)
+        restore(i)
+    ctx.synchronize()
+    for i in range(len(slots)):
+        restore(i)
+    torch.cuda.synchronize()
+
+    hbm, peak_kind = peaks()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ctx.profile(True)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for i in range(args.steps):
+        evs[i][0].record(s)
+        step(i)
+        evs[i][1].record(s)
+        restore(i)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+
+    value = n * args.steps * world / (total_ms / 1e3) / 1e9
+    ms_per_step = total_ms / args.steps
+
+    # roofline of the dominant kernel (the onesweep digit pass): algorithmic bytes per
+    # launch = one read + one write of the keys = 2 * n * w
+    os_launches, os_ms = prof["onesweep"]
+    os_avg_ms = os_ms / max(1, os_launches)
+    os_bytes = 2.0 * n * w
+    achieved = os_bytes / (os_avg_ms / 1e3) / 1e9 if os_launches else None
+    roof = {"kernel": "onesweep_pass", "bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
+            "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": round(achieved / hbm, 4) if achieved else None,
+            "traffic": read_traffic(dtype), "algorithmic_bytes_per_launch": os_bytes,
+            "avg_launch_ms": round(os_avg_ms, 5), "launches": os_launches}
+    sort_bytes = n * w * (1 + 2 * P)
+    sort_achieved = sort_bytes / (ms_per_step / 1e3) / 1e9
+    sort_roof = {"bytes_per_step": sort_bytes, "achieved": round(sort_achieved, 1), "peak": hbm,
+                 "unit": "GB/s", "frac": round(sort_achieved / hbm, 4),
+                 "kernels_ms_per_step": {k: round(v[1] / args.steps, 5) for k, v in prof.items() if v[0]}}
+    launches = sum(v[0] for v in prof.values())
+
+    # end to end through the host-array C ABI call (pinned host memory)
+    e2e = None
+    if not args.no_e2e:
+        ksteps = args.e2e_steps or min(args.steps, 20)
+        pinned = torch.empty(n, dtype=tview, pin_memory=True)
+        pn = pinned.numpy().view(host.dtype)
+        lib = native.load()
+        fn = getattr(lib, f"hpcs_sort_{dtype}")
+        np.copyto(pn, host)
+        native.check(fn(ctx.handle, pn.ctypes.data, n))  # warm
+        tot = 0.0
+        for _ in range(ksteps):
+            np.copyto(pn, host)
+            if dist:
+                dist.barrier()
+            t0 = time.perf_counter()
+            native.check(fn(ctx.handle, pn.ctypes.data, n))
+            tot += time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([tot], device=f"cuda:{dev}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tot = float(t.item())
+        e2e = {"value": round(n * ksteps * world / tot / 1e9, 4), "unit": UNIT,
+               "h2d_bytes_per_step": n * w, "d2h_bytes_per_step": n * w, "steps": ksteps,
+               "ms_per_step": round(tot / ksteps * 1e3, 3), "api": f"hpcs_sort_{dtype} (host array, pinned)"}
+        # the last e2e result must be in order
+        if not _in_order(pn):
+            raise RuntimeError("e2e result is not sorted")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(dtype, n)
+
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+            "data": "synthetic (seeded PCG32 uniform keys)",
+            "config": {"workload": f"plain LSD radix sort of {n} {dtype} keys uniform over the key range, "
+                                   f"device-resident, stable, 8-bit digits",
+                       "n": n, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (1 GiB per copy); input restored between steps"},
+            "roofline": roof, "sort_roofline": sort_roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,82 @@
+"""Build recipe for the native parts of hpcsharp_b200.
+
+Outputs (all in-tree, git-ignored, shipped with the tree):
+  hpcsharp_b200/libhpcs_gpu.so   CUDA kernels + C ABI (include/hpcs_gpu.h), sm_100a only
+  hpcsharp_b200/libhpcs_gen.so   seeded synthetic key generators (host C++)
+
+nvcc cross-compiles for sm_100a without a GPU.  Run: python -m hpcsharp_b200.build
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17",
+    "-Xcompiler", "-fPIC", "-shared",
+    "-Xptxas", "-warn-spills",
+    "--expt-relaxed-constexpr",
+]
+
+GPU_SOURCES = ["capi.cu"]
+GPU_DEPS = ["common.cuh", "radix_kernels.cuh", "sort_host.cuh"]
+
+
+def _nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(target: str, sources: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def _run(cmd: list[str]) -> None:
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("build step failed: " + " ".join(cmd[:3]) + " ...")
+    if res.stderr.strip():
+        sys.stderr.write(res.stderr)
+
+
+def build_gpu(force: bool = False, verbose_ptxas: bool = False) -> str:
+    out = os.path.join(PKG, "libhpcs_gpu.so")
+    srcs = [os.path.join(CSRC, s) for s in GPU_SOURCES]
+    deps = srcs + [os.path.join(CSRC, d) for d in GPU_DEPS] + [os.path.join(ROOT, "include", "hpcs_gpu.h")]
+    if force or _stale(out, deps):
+        flags = list(NVCC_FLAGS)
+        if verbose_ptxas:
+            flags += ["-Xptxas", "-v"]
+        _run([_nvcc(), *flags, "-o", out, *srcs])
+    return out
+
+
+def build_gen(force: bool = False) -> str:
+    out = os.path.join(PKG, "libhpcs_gen.so")
+    src = os.path.join(PKG, "datagen", "gen.cpp")
+    if force or _stale(out, [src]):
+        _run(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-pthread", "-o", out, src])
+    return out
+
+
+def build_all(force: bool = False) -> None:
+    build_gen(force)
+    build_gpu(force)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv)
+    print("built", os.path.join(PKG, "libhpcs_gpu.so"), os.path.join(PKG, "libhpcs_gen.so"))

@@ -1,0 +1,480 @@
+// C ABI of libhpcs_gpu.so (declared in include/hpcs_gpu.h): contexts, argument checks that
+// mirror the reference's exceptions, host-array and device-pointer entry points.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <string>
+
+#include "../../include/hpcs_gpu.h"
+#include "sort_host.cuh"
+
+namespace hpcs {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int status, const std::string& msg) {
+  set_error(msg);
+  return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return fail(HPCS_ERR_OOM, m);
+  return fail(HPCS_ERR_CUDA, m);
+}
+
+int ensure(hpcs_ctx* ctx, DevBuf& b, size_t bytes) {
+  if (b.bytes >= bytes) return HPCS_OK;
+  size_t want = bytes < 256 ? 256 : bytes;
+  if (ctx->cfg.pool_bytes > 0 && ctx->held_bytes - b.bytes + want > size_t(ctx->cfg.pool_bytes))
+    return fail(HPCS_ERR_OOM, "request exceeds the context's pool_bytes budget");
+  if (b.ptr) {
+    // earlier work on the context's streams may still read the old buffer
+    cudaError_t e = cudaStreamSynchronize(ctx->last_stream ? ctx->last_stream : ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    cudaFree(b.ptr);
+    ctx->held_bytes -= b.bytes;
+    b.ptr = nullptr;
+    b.bytes = 0;
+  }
+  cudaError_t e = cudaMalloc(&b.ptr, want);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    b.ptr = nullptr;
+    return cuda_fail(e, "cudaMalloc");
+  }
+  b.bytes = want;
+  ctx->held_bytes += want;
+  return HPCS_OK;
+}
+
+int enter_stream(hpcs_ctx* ctx, cudaStream_t s) {
+  if (ctx->last_stream != nullptr && ctx->last_stream != s) {
+    HPCS_CUDA(cudaEventRecord(ctx->order_event, ctx->last_stream));
+    HPCS_CUDA(cudaStreamWaitEvent(s, ctx->order_event, 0));
+  }
+  ctx->last_stream = s;
+  return HPCS_OK;
+}
+
+static cudaEvent_t take_event(hpcs_ctx* ctx) {
+  if (!ctx->event_pool.empty()) {
+    cudaEvent_t e = ctx->event_pool.back();
+    ctx->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return e;
+}
+
+KernelTimer::KernelTimer(hpcs_ctx* c, cudaStream_t st, int k) : ctx(c), s(st), cls(k) {
+  if (!ctx->profile) return;
+  a = take_event(ctx);
+  b = take_event(ctx);
+  if (a) cudaEventRecord(a, s);
+}
+
+KernelTimer::~KernelTimer() {
+  if (!ctx->profile || !a || !b) return;
+  cudaEventRecord(b, s);
+  ctx->timed.push_back({cls, a, b});
+}
+
+uint32_t* device_error_word(hpcs_ctx* ctx) { return static_cast<uint32_t*>(ctx->err_accum.ptr); }
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+cudaStream_t pick_stream(hpcs_ctx* ctx, void* stream) {
+  return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+}
+
+// Reads and clears the accumulated device error bits (synchronous).
+int check_device_errors(hpcs_ctx* ctx) {
+  uint32_t bits = 0;
+  HPCS_CUDA(cudaMemcpy(&bits, ctx->err_accum.ptr, 4, cudaMemcpyDeviceToHost));
+  if (bits) {
+    HPCS_CUDA(cudaMemset(ctx->err_accum.ptr, 0, 4));
+    char buf[160];
+    std::snprintf(buf, sizeof buf,
+                  "device-side wait ran out (error bits 0x%x: 1=look-back, 2=bulk copy, 4=bounds, 8=queue)",
+                  bits);
+    return fail(HPCS_ERR_DEVICE_TIMEOUT, buf);
+  }
+  return HPCS_OK;
+}
+
+int check_common(hpcs_ctx* ctx, const void* p, int64_t n) {
+  if (!ctx) return fail(HPCS_ERR_NULL, "ctx is NULL");
+  if (!p) return fail(HPCS_ERR_NULL, "array is NULL");
+  if (n < 0) return fail(HPCS_ERR_RANGE, "length is negative");
+  if (n > HPCS_MAX_KEYS) return fail(HPCS_ERR_RANGE, "length exceeds HPCS_MAX_KEYS");
+  return HPCS_OK;
+}
+
+template <class T, class U, int KIND>
+int sort_host(hpcs_ctx* ctx, T* keys, int64_t n) {
+  int rc = check_common(ctx, keys, n);
+  if (rc != HPCS_OK || n == 0) return rc;
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = ctx->stream;
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->keys_a, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
+  U* d = static_cast<U*>(ctx->keys_a.ptr);
+  HPCS_CUDA(cudaMemcpyAsync(d, keys, size_t(n) * sizeof(U), cudaMemcpyHostToDevice, s));
+  if ((rc = enqueue_sort<U, KIND, NoValue>(ctx, d, nullptr, n, s)) != HPCS_OK) return rc;
+  HPCS_CUDA(cudaMemcpyAsync(keys, d, size_t(n) * sizeof(U), cudaMemcpyDeviceToHost, s));
+  HPCS_CUDA(cudaStreamSynchronize(s));
+  return check_device_errors(ctx);
+}
+
+template <class T, class U, int KIND>
+int sort_dev(hpcs_ctx* ctx, T* keys, int64_t n, void* stream) {
+  int rc = check_common(ctx, keys, n);
+  if (rc != HPCS_OK || n == 0) return rc;
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = pick_stream(ctx, stream);
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  return enqueue_sort<U, KIND, NoValue>(ctx, reinterpret_cast<U*>(keys), nullptr, n, s);
+}
+
+template <class T, class U, int KIND>
+int pairs_host(hpcs_ctx* ctx, T* keys, uint32_t* items, int64_t n) {
+  int rc = check_common(ctx, keys, n);
+  if (rc != HPCS_OK) return rc;
+  if (!items) return fail(HPCS_ERR_NULL, "items is NULL");
+  if (n == 0) return HPCS_OK;
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = ctx->stream;
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->keys_a, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->vals_a, size_t(n) * 4)) != HPCS_OK) return rc;
+  U* dk = static_cast<U*>(ctx->keys_a.ptr);
+  uint32_t* dv = static_cast<uint32_t*>(ctx->vals_a.ptr);
+  HPCS_CUDA(cudaMemcpyAsync(dk, keys, size_t(n) * sizeof(U), cudaMemcpyHostToDevice, s));
+  HPCS_CUDA(cudaMemcpyAsync(dv, items, size_t(n) * 4, cudaMemcpyHostToDevice, s));
+  if ((rc = enqueue_sort<U, KIND, uint32_t>(ctx, dk, dv, n, s)) != HPCS_OK) return rc;
+  HPCS_CUDA(cudaMemcpyAsync(keys, dk, size_t(n) * sizeof(U), cudaMemcpyDeviceToHost, s));
+  HPCS_CUDA(cudaMemcpyAsync(items, dv, size_t(n) * 4, cudaMemcpyDeviceToHost, s));
+  HPCS_CUDA(cudaStreamSynchronize(s));
+  return check_device_errors(ctx);
+}
+
+template <class T, class U, int KIND>
+int pairs_dev(hpcs_ctx* ctx, T* keys, uint32_t* items, int64_t n, void* stream) {
+  int rc = check_common(ctx, keys, n);
+  if (rc != HPCS_OK) return rc;
+  if (!items) return fail(HPCS_ERR_NULL, "items is NULL");
+  if (n == 0) return HPCS_OK;
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = pick_stream(ctx, stream);
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  return enqueue_sort<U, KIND, uint32_t>(ctx, reinterpret_cast<U*>(keys), items, n, s);
+}
+
+// Histogram of n keys at device pointer d into device counts[P][256] (zeroed here).
+template <class U, int KIND>
+int enqueue_histogram(hpcs_ctx* ctx, const U* d, int64_t n, uint32_t* counts, cudaStream_t s) {
+  constexpr int P = int(sizeof(U));
+  HPCS_CUDA(cudaMemsetAsync(counts, 0, size_t(P) * RADIX * 4, s));
+  if (n <= 0) return HPCS_OK;
+  const U* src = d;
+  int rc;
+  if ((reinterpret_cast<uintptr_t>(d) & 15) != 0) {  // the vector loads need 16-byte alignment
+    if ((rc = ensure(ctx, ctx->keys_b, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
+    HPCS_CUDA(cudaMemcpyAsync(ctx->keys_b.ptr, d, size_t(n) * sizeof(U), cudaMemcpyDeviceToDevice, s));
+    src = static_cast<const U*>(ctx->keys_b.ptr);
+  }
+  auto k = hist_all_digits_kernel<U, KIND, HIST_NT>;
+  static int blocks = 0;
+  if (!blocks) blocks = occupancy_blocks(k, HIST_NT, 0);
+  const int64_t vec = n * int64_t(sizeof(U)) / 16;
+  int64_t want = (vec + HIST_NT * 4 - 1) / (HIST_NT * 4);
+  int64_t cap = int64_t(ctx->sms) * blocks;
+  int grid = int(want < 1 ? 1 : (want > cap ? cap : want));
+  SortArgs none{};
+  k<<<grid, HIST_NT, 0, s>>>(src, n, counts, none, 0);
+  HPCS_CUDA(cudaGetLastError());
+  return HPCS_OK;
+}
+
+template <class T, class U, int KIND>
+int histogram_host(hpcs_ctx* ctx, const T* a, int64_t l, int64_t r, uint32_t* counts) {
+  constexpr int P = int(sizeof(U));
+  if (!ctx) return fail(HPCS_ERR_NULL, "ctx is NULL");
+  if (!a) return fail(HPCS_ERR_NULL, "array is NULL");
+  if (!counts) return fail(HPCS_ERR_NULL, "counts is NULL");
+  if (l < 0) return fail(HPCS_ERR_RANGE, "l is negative");
+  const int64_t n = r - l + 1;
+  if (n > HPCS_MAX_KEYS) return fail(HPCS_ERR_RANGE, "range exceeds HPCS_MAX_KEYS");
+  if (n <= 0) {
+    std::memset(counts, 0, size_t(P) * RADIX * 4);
+    return HPCS_OK;
+  }
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = ctx->stream;
+  int rc;
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->keys_a, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->counts, size_t(MAX_PASSES) * RADIX * 4)) != HPCS_OK) return rc;
+  U* d = static_cast<U*>(ctx->keys_a.ptr);
+  uint32_t* dc = static_cast<uint32_t*>(ctx->counts.ptr);
+  HPCS_CUDA(cudaMemcpyAsync(d, a + l, size_t(n) * sizeof(U), cudaMemcpyHostToDevice, s));
+  if ((rc = enqueue_histogram<U, KIND>(ctx, d, n, dc, s)) != HPCS_OK) return rc;
+  HPCS_CUDA(cudaMemcpyAsync(counts, dc, size_t(P) * RADIX * 4, cudaMemcpyDeviceToHost, s));
+  HPCS_CUDA(cudaStreamSynchronize(s));
+  return HPCS_OK;
+}
+
+}  // namespace
+}  // namespace hpcs
+
+using namespace hpcs;
+
+extern "C" {
+
+void hpcs_config_default(hpcs_config* cfg) {
+  if (!cfg) return;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->pool_bytes = 0;
+  cfg->skip_trivial_passes = 1;
+  cfg->spin_limit_ns = 2000000000LL;
+  cfg->poison_tile = -1;
+}
+
+int hpcs_abi_version(void) { return HPCS_ABI_VERSION; }
+
+const char* hpcs_last_error_message(void) { return g_last_error.c_str(); }
+
+const char* hpcs_status_string(int status) {
+  switch (status) {
+    case HPCS_OK: return "HPCS_OK";
+    case HPCS_ERR_NULL: return "HPCS_ERR_NULL";
+    case HPCS_ERR_RANGE: return "HPCS_ERR_RANGE";
+    case HPCS_ERR_OOM: return "HPCS_ERR_OOM";
+    case HPCS_ERR_CUDA: return "HPCS_ERR_CUDA";
+    case HPCS_ERR_DEVICE_TIMEOUT: return "HPCS_ERR_DEVICE_TIMEOUT";
+    case HPCS_ERR_UNSUPPORTED: return "HPCS_ERR_UNSUPPORTED";
+    case HPCS_ERR_NO_DEVICE: return "HPCS_ERR_NO_DEVICE";
+    case HPCS_ERR_BUSY: return "HPCS_ERR_BUSY";
+    default: return "HPCS_ERR_UNKNOWN";
+  }
+}
+
+int hpcs_ctx_create(int device, const hpcs_config* cfg, hpcs_ctx** out) {
+  if (!out) return fail(HPCS_ERR_NULL, "out is NULL");
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return fail(HPCS_ERR_NO_DEVICE, "no CUDA device is available");
+  }
+  if (device < 0 || device >= count) return fail(HPCS_ERR_RANGE, "device index out of range");
+  DeviceGuard g(device);
+  auto* ctx = new hpcs_ctx();
+  ctx->device = device;
+  if (cfg) ctx->cfg = *cfg;
+  else hpcs_config_default(&ctx->cfg);
+  if (ctx->cfg.spin_limit_ns <= 0) ctx->cfg.spin_limit_ns = 2000000000LL;
+  cudaDeviceProp prop{};
+  if ((e = cudaGetDeviceProperties(&prop, device)) != cudaSuccess) {
+    delete ctx;
+    return cuda_fail(e, "cudaGetDeviceProperties");
+  }
+  if (prop.major < 10) {
+    delete ctx;
+    return fail(HPCS_ERR_UNSUPPORTED, "libhpcs_gpu is built for sm_100a (B200)");
+  }
+  ctx->sms = prop.multiProcessorCount;
+  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&ctx->order_event, cudaEventDisableTiming)) != cudaSuccess) {
+    delete ctx;
+    return cuda_fail(e, "stream/event create");
+  }
+  int rc = ensure(ctx, ctx->err_accum, 256);
+  if (rc != HPCS_OK || cudaMemset(ctx->err_accum.ptr, 0, 256) != cudaSuccess) {
+    hpcs_ctx_destroy(ctx);
+    return rc != HPCS_OK ? rc : fail(HPCS_ERR_CUDA, "cudaMemset");
+  }
+  *out = ctx;
+  return HPCS_OK;
+}
+
+int hpcs_ctx_destroy(hpcs_ctx* ctx) {
+  if (!ctx) return HPCS_OK;
+  DeviceGuard g(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->last_stream && ctx->last_stream != ctx->stream) cudaStreamSynchronize(ctx->last_stream);
+  DevBuf* bufs[] = {&ctx->keys_a, &ctx->keys_b, &ctx->vals_a, &ctx->vals_b, &ctx->status0, &ctx->status1,
+                    &ctx->plan,   &ctx->counts, &ctx->err_accum, &ctx->aux0, &ctx->aux1, &ctx->aux2};
+  for (DevBuf* b : bufs)
+    if (b->ptr) cudaFree(b->ptr);
+  for (auto& t : ctx->timed) {
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+  if (ctx->order_event) cudaEventDestroy(ctx->order_event);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return HPCS_OK;
+}
+
+int hpcs_ctx_synchronize(hpcs_ctx* ctx) {
+  if (!ctx) return fail(HPCS_ERR_NULL, "ctx is NULL");
+  DeviceGuard g(ctx->device);
+  HPCS_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (ctx->last_stream && ctx->last_stream != ctx->stream) HPCS_CUDA(cudaStreamSynchronize(ctx->last_stream));
+  return check_device_errors(ctx);
+}
+
+int hpcs_ctx_profile_enable(hpcs_ctx* ctx, int enable) {
+  if (!ctx) return fail(HPCS_ERR_NULL, "ctx is NULL");
+  ctx->profile = enable != 0;
+  return HPCS_OK;
+}
+
+int hpcs_ctx_profile_read(hpcs_ctx* ctx, hpcs_profile* out) {
+  if (!ctx || !out) return fail(HPCS_ERR_NULL, "ctx or out is NULL");
+  DeviceGuard g(ctx->device);
+  std::memset(out, 0, sizeof(*out));
+  for (auto& t : ctx->timed) {
+    HPCS_CUDA(cudaEventSynchronize(t.b));
+    float ms = 0.f;
+    HPCS_CUDA(cudaEventElapsedTime(&ms, t.a, t.b));
+    if (t.cls >= 0 && t.cls < HPCS_K_CLASSES) {
+      out->launches[t.cls] += 1;
+      out->total_ms[t.cls] += ms;
+    }
+    ctx->event_pool.push_back(t.a);
+    ctx->event_pool.push_back(t.b);
+  }
+  ctx->timed.clear();
+  return HPCS_OK;
+}
+
+void* hpcs_ctx_stream(hpcs_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+// ---- plain sorts ----
+int hpcs_sort_u32(hpcs_ctx* c, uint32_t* k, int64_t n) { return sort_host<uint32_t, uint32_t, KIND_UNSIGNED>(c, k, n); }
+int hpcs_sort_i32(hpcs_ctx* c, int32_t* k, int64_t n) { return sort_host<int32_t, uint32_t, KIND_SIGNED>(c, k, n); }
+int hpcs_sort_f32(hpcs_ctx* c, float* k, int64_t n) { return sort_host<float, uint32_t, KIND_FLOAT>(c, k, n); }
+int hpcs_sort_u64(hpcs_ctx* c, uint64_t* k, int64_t n) { return sort_host<uint64_t, uint64_t, KIND_UNSIGNED>(c, k, n); }
+int hpcs_sort_i64(hpcs_ctx* c, int64_t* k, int64_t n) { return sort_host<int64_t, uint64_t, KIND_SIGNED>(c, k, n); }
+int hpcs_sort_f64(hpcs_ctx* c, double* k, int64_t n) { return sort_host<double, uint64_t, KIND_FLOAT>(c, k, n); }
+
+int hpcs_sort_u32_dev(hpcs_ctx* c, uint32_t* k, int64_t n, void* s) {
+  return sort_dev<uint32_t, uint32_t, KIND_UNSIGNED>(c, k, n, s);
+}
+int hpcs_sort_i32_dev(hpcs_ctx* c, int32_t* k, int64_t n, void* s) {
+  return sort_dev<int32_t, uint32_t, KIND_SIGNED>(c, k, n, s);
+}
+int hpcs_sort_f32_dev(hpcs_ctx* c, float* k, int64_t n, void* s) { return sort_dev<float, uint32_t, KIND_FLOAT>(c, k, n, s); }
+int hpcs_sort_u64_dev(hpcs_ctx* c, uint64_t* k, int64_t n, void* s) {
+  return sort_dev<uint64_t, uint64_t, KIND_UNSIGNED>(c, k, n, s);
+}
+int hpcs_sort_i64_dev(hpcs_ctx* c, int64_t* k, int64_t n, void* s) {
+  return sort_dev<int64_t, uint64_t, KIND_SIGNED>(c, k, n, s);
+}
+int hpcs_sort_f64_dev(hpcs_ctx* c, double* k, int64_t n, void* s) {
+  return sort_dev<double, uint64_t, KIND_FLOAT>(c, k, n, s);
+}
+
+// ---- pairs ----
+int hpcs_sort_pairs_u32(hpcs_ctx* c, uint32_t* k, uint32_t* v, int64_t n) {
+  return pairs_host<uint32_t, uint32_t, KIND_UNSIGNED>(c, k, v, n);
+}
+int hpcs_sort_pairs_i32(hpcs_ctx* c, int32_t* k, uint32_t* v, int64_t n) {
+  return pairs_host<int32_t, uint32_t, KIND_SIGNED>(c, k, v, n);
+}
+int hpcs_sort_pairs_f32(hpcs_ctx* c, float* k, uint32_t* v, int64_t n) {
+  return pairs_host<float, uint32_t, KIND_FLOAT>(c, k, v, n);
+}
+int hpcs_sort_pairs_u64(hpcs_ctx* c, uint64_t* k, uint32_t* v, int64_t n) {
+  return pairs_host<uint64_t, uint64_t, KIND_UNSIGNED>(c, k, v, n);
+}
+int hpcs_sort_pairs_i64(hpcs_ctx* c, int64_t* k, uint32_t* v, int64_t n) {
+  return pairs_host<int64_t, uint64_t, KIND_SIGNED>(c, k, v, n);
+}
+int hpcs_sort_pairs_f64(hpcs_ctx* c, double* k, uint32_t* v, int64_t n) {
+  return pairs_host<double, uint64_t, KIND_FLOAT>(c, k, v, n);
+}
+int hpcs_sort_pairs_u32_dev(hpcs_ctx* c, uint32_t* k, uint32_t* v, int64_t n, void* s) {
+  return pairs_dev<uint32_t, uint32_t, KIND_UNSIGNED>(c, k, v, n, s);
+}
+int hpcs_sort_pairs_i32_dev(hpcs_ctx* c, int32_t* k, uint32_t* v, int64_t n, void* s) {
+  return pairs_dev<int32_t, uint32_t, KIND_SIGNED>(c, k, v, n, s);
+}
+int hpcs_sort_pairs_f32_dev(hpcs_ctx* c, float* k, uint32_t* v, int64_t n, void* s) {
+  return pairs_dev<float, uint32_t, KIND_FLOAT>(c, k, v, n, s);
+}
+int hpcs_sort_pairs_u64_dev(hpcs_ctx* c, uint64_t* k, uint32_t* v, int64_t n, void* s) {
+  return pairs_dev<uint64_t, uint64_t, KIND_UNSIGNED>(c, k, v, n, s);
+}
+int hpcs_sort_pairs_i64_dev(hpcs_ctx* c, int64_t* k, uint32_t* v, int64_t n, void* s) {
+  return pairs_dev<int64_t, uint64_t, KIND_SIGNED>(c, k, v, n, s);
+}
+int hpcs_sort_pairs_f64_dev(hpcs_ctx* c, double* k, uint32_t* v, int64_t n, void* s) {
+  return pairs_dev<double, uint64_t, KIND_FLOAT>(c, k, v, n, s);
+}
+
+// ---- histograms ----
+int hpcs_histogram_byte_components_u32(hpcs_ctx* c, const uint32_t* a, int64_t l, int64_t r, uint32_t* o) {
+  return histogram_host<uint32_t, uint32_t, KIND_UNSIGNED>(c, a, l, r, o);
+}
+int hpcs_histogram_byte_components_i32(hpcs_ctx* c, const int32_t* a, int64_t l, int64_t r, uint32_t* o) {
+  return histogram_host<int32_t, uint32_t, KIND_SIGNED>(c, a, l, r, o);
+}
+int hpcs_histogram_byte_components_f32(hpcs_ctx* c, const float* a, int64_t l, int64_t r, uint32_t* o) {
+  return histogram_host<float, uint32_t, KIND_FLOAT>(c, a, l, r, o);
+}
+int hpcs_histogram_byte_components_u64(hpcs_ctx* c, const uint64_t* a, int64_t l, int64_t r, uint32_t* o) {
+  return histogram_host<uint64_t, uint64_t, KIND_UNSIGNED>(c, a, l, r, o);
+}
+int hpcs_histogram_byte_components_i64(hpcs_ctx* c, const int64_t* a, int64_t l, int64_t r, uint32_t* o) {
+  return histogram_host<int64_t, uint64_t, KIND_SIGNED>(c, a, l, r, o);
+}
+int hpcs_histogram_byte_components_f64(hpcs_ctx* c, const double* a, int64_t l, int64_t r, uint32_t* o) {
+  return histogram_host<double, uint64_t, KIND_FLOAT>(c, a, l, r, o);
+}
+
+int hpcs_histogram_byte_components_dev(hpcs_ctx* ctx, int dtype, const void* a, int64_t n, uint32_t* counts,
+                                       void* stream) {
+  int rc = check_common(ctx, a, n);
+  if (rc != HPCS_OK) return rc;
+  if (!counts) return fail(HPCS_ERR_NULL, "counts is NULL");
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = pick_stream(ctx, stream);
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  switch (dtype) {
+    case HPCS_U32: return enqueue_histogram<uint32_t, KIND_UNSIGNED>(ctx, static_cast<const uint32_t*>(a), n, counts, s);
+    case HPCS_I32: return enqueue_histogram<uint32_t, KIND_SIGNED>(ctx, static_cast<const uint32_t*>(a), n, counts, s);
+    case HPCS_F32: return enqueue_histogram<uint32_t, KIND_FLOAT>(ctx, static_cast<const uint32_t*>(a), n, counts, s);
+    case HPCS_U64: return enqueue_histogram<uint64_t, KIND_UNSIGNED>(ctx, static_cast<const uint64_t*>(a), n, counts, s);
+    case HPCS_I64: return enqueue_histogram<uint64_t, KIND_SIGNED>(ctx, static_cast<const uint64_t*>(a), n, counts, s);
+    case HPCS_F64: return enqueue_histogram<uint64_t, KIND_FLOAT>(ctx, static_cast<const uint64_t*>(a), n, counts, s);
+    default: return fail(HPCS_ERR_UNSUPPORTED, "unknown dtype");
+  }
+}
+
+}  // extern "C"

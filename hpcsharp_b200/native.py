@@ -1,0 +1,267 @@
+"""ctypes bindings of libhpcs_gpu.so (the C ABI declared in include/hpcs_gpu.h).
+
+This module is plumbing for Python callers (tests, benchmarks, the serving demo); the
+compute path is the CUDA library.  There is no CPU fallback: if the library or a CUDA
+device is missing, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libhpcs_gpu.so")
+
+HPCS_OK = 0
+HPCS_ERR_NULL = 1
+HPCS_ERR_RANGE = 2
+HPCS_ERR_OOM = 3
+HPCS_ERR_CUDA = 4
+HPCS_ERR_DEVICE_TIMEOUT = 5
+HPCS_ERR_UNSUPPORTED = 6
+HPCS_ERR_NO_DEVICE = 7
+HPCS_ERR_BUSY = 8
+
+DTYPES = {"u32": 0, "i32": 1, "f32": 2, "u64": 3, "i64": 4, "f64": 5}
+NP_OF = {"u32": np.uint32, "i32": np.int32, "f32": np.float32, "u64": np.uint64, "i64": np.int64, "f64": np.float64}
+CT_OF = {"u32": C.c_uint32, "i32": C.c_int32, "f32": C.c_float, "u64": C.c_uint64, "i64": C.c_int64,
+         "f64": C.c_double}
+
+
+def dtype_name(arr_dtype) -> str:
+    dt = np.dtype(arr_dtype)
+    for k, v in NP_OF.items():
+        if np.dtype(v) == dt:
+            return k
+    raise TypeError(f"unsupported key dtype {dt}")
+
+
+class HpcsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_status_name(status)}: {message}")
+        self.status = status
+
+
+class ArgumentNullException(HpcsError, ValueError):
+    """Raised for HPCS_ERR_NULL (the reference throws ArgumentNullException)."""
+
+
+class ArgumentOutOfRangeException(HpcsError, IndexError):
+    """Raised for HPCS_ERR_RANGE (the reference throws ArgumentOutOfRangeException)."""
+
+
+class DeviceTimeoutError(HpcsError):
+    """A bounded device-side wait ran out (HPCS_ERR_DEVICE_TIMEOUT)."""
+
+
+class HpcsConfig(C.Structure):
+    _fields_ = [
+        ("pool_bytes", C.c_int64),
+        ("skip_trivial_passes", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("spin_limit_ns", C.c_int64),
+        ("poison_tile", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+
+KCLASS = {"histogram": 0, "onesweep": 1, "finalize": 2, "topk": 3, "segmented": 4}
+
+
+class HpcsProfile(C.Structure):
+    _fields_ = [("launches", C.c_int64 * 8), ("total_ms", C.c_double * 8)]
+
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def _status_name(status: int) -> str:
+    names = {0: "HPCS_OK", 1: "HPCS_ERR_NULL", 2: "HPCS_ERR_RANGE", 3: "HPCS_ERR_OOM", 4: "HPCS_ERR_CUDA",
+             5: "HPCS_ERR_DEVICE_TIMEOUT", 6: "HPCS_ERR_UNSUPPORTED", 7: "HPCS_ERR_NO_DEVICE", 8: "HPCS_ERR_BUSY"}
+    return names.get(status, f"status {status}")
+
+
+def _declare(lib) -> None:
+    P, I64, I32, U32P = C.c_void_p, C.c_int64, C.c_int, C.POINTER(C.c_uint32)
+    lib.hpcs_config_default.argtypes = [C.POINTER(HpcsConfig)]
+    lib.hpcs_config_default.restype = None
+    lib.hpcs_ctx_create.argtypes = [I32, C.POINTER(HpcsConfig), C.POINTER(P)]
+    lib.hpcs_ctx_destroy.argtypes = [P]
+    lib.hpcs_ctx_synchronize.argtypes = [P]
+    lib.hpcs_ctx_stream.argtypes = [P]
+    lib.hpcs_ctx_stream.restype = P
+    lib.hpcs_last_error_message.restype = C.c_char_p
+    lib.hpcs_status_string.argtypes = [I32]
+    lib.hpcs_status_string.restype = C.c_char_p
+    for t in DTYPES:
+        getattr(lib, f"hpcs_sort_{t}").argtypes = [P, P, I64]
+        getattr(lib, f"hpcs_sort_{t}_dev").argtypes = [P, P, I64, P]
+        getattr(lib, f"hpcs_sort_pairs_{t}").argtypes = [P, P, P, I64]
+        getattr(lib, f"hpcs_sort_pairs_{t}_dev").argtypes = [P, P, P, I64, P]
+        getattr(lib, f"hpcs_histogram_byte_components_{t}").argtypes = [P, P, I64, I64, P]
+    lib.hpcs_histogram_byte_components_dev.argtypes = [P, I32, P, I64, P, P]
+    lib.hpcs_ctx_profile_enable.argtypes = [P, I32]
+    lib.hpcs_ctx_profile_read.argtypes = [P, C.POINTER(HpcsProfile)]
+
+
+def load():
+    """Load libhpcs_gpu.so (raises if it was not built)."""
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(f"{LIB_PATH} is missing; run `python -m hpcsharp_b200.build`")
+            lib = C.CDLL(LIB_PATH)
+            _declare(lib)
+            _lib = lib
+    return _lib
+
+
+def check(status: int) -> None:
+    if status == HPCS_OK:
+        return
+    msg = load().hpcs_last_error_message().decode(errors="replace")
+    if status == HPCS_ERR_NULL:
+        raise ArgumentNullException(status, msg)
+    if status == HPCS_ERR_RANGE:
+        raise ArgumentOutOfRangeException(status, msg)
+    if status == HPCS_ERR_DEVICE_TIMEOUT:
+        raise DeviceTimeoutError(status, msg)
+    raise HpcsError(status, msg)
+
+
+def default_config() -> HpcsConfig:
+    cfg = HpcsConfig()
+    load().hpcs_config_default(C.byref(cfg))
+    return cfg
+
+
+def _ptr(a) -> int | None:
+    """Address of a numpy array (host) or a torch tensor (device)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags.c_contiguous:
+            raise ValueError("array must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return a.data_ptr()
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+class Context:
+    """One hpcs_ctx: a CUDA stream plus grow-only scratch on one device."""
+
+    def __init__(self, device: int = 0, *, pool_bytes: int = 0, skip_trivial_passes: bool = True,
+                 spin_limit_ns: int = 2_000_000_000, poison_tile: int = -1):
+        self.lib = load()
+        cfg = default_config()
+        cfg.pool_bytes = pool_bytes
+        cfg.skip_trivial_passes = 1 if skip_trivial_passes else 0
+        cfg.spin_limit_ns = spin_limit_ns
+        cfg.poison_tile = poison_tile
+        h = C.c_void_p()
+        check(self.lib.hpcs_ctx_create(device, C.byref(cfg), C.byref(h)))
+        self.handle = h
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.hpcs_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def stream(self) -> int:
+        return self.lib.hpcs_ctx_stream(self.handle) or 0
+
+    def synchronize(self) -> None:
+        check(self.lib.hpcs_ctx_synchronize(self.handle))
+
+    def profile(self, enable: bool = True) -> None:
+        """Record a CUDA event pair around every kernel this context launches."""
+        check(self.lib.hpcs_ctx_profile_enable(self.handle, 1 if enable else 0))
+
+    def profile_read(self) -> dict:
+        """{kernel class: (launches, total ms)} since the last read (waits for the GPU)."""
+        p = HpcsProfile()
+        check(self.lib.hpcs_ctx_profile_read(self.handle, C.byref(p)))
+        return {k: (int(p.launches[v]), float(p.total_ms[v])) for k, v in KCLASS.items()}
+
+    # ---- host arrays (synchronous, in place) ----
+    def sort(self, a: np.ndarray) -> np.ndarray:
+        t = dtype_name(a.dtype)
+        check(getattr(self.lib, f"hpcs_sort_{t}")(self.handle, _ptr(a), a.size))
+        return a
+
+    def sort_pairs(self, keys: np.ndarray, items: np.ndarray):
+        t = dtype_name(keys.dtype)
+        if items is not None and items.dtype.itemsize != 4:
+            raise TypeError("items must be 4-byte")
+        if items is not None and items.size != keys.size:
+            raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "keys and items differ in length")
+        check(getattr(self.lib, f"hpcs_sort_pairs_{t}")(self.handle, _ptr(keys), _ptr(items), keys.size))
+        return keys, items
+
+    def histogram(self, a: np.ndarray, l: int, r: int) -> np.ndarray:
+        t = dtype_name(a.dtype)
+        P = a.dtype.itemsize
+        counts = np.zeros((P, 256), dtype=np.uint32)
+        check(getattr(self.lib, f"hpcs_histogram_byte_components_{t}")(self.handle, _ptr(a), l, r, _ptr(counts)))
+        return counts
+
+    # ---- device tensors (asynchronous on `stream`, default: the context's stream) ----
+    def sort_dev(self, t, dtype: str | None = None, stream: int | None = None) -> None:
+        name = dtype or _torch_dtype_name(t)
+        check(getattr(self.lib, f"hpcs_sort_{name}_dev")(self.handle, _ptr(t), t.numel(), stream))
+
+    def sort_pairs_dev(self, keys, items, dtype: str | None = None, stream: int | None = None) -> None:
+        name = dtype or _torch_dtype_name(keys)
+        check(getattr(self.lib, f"hpcs_sort_pairs_{name}_dev")(self.handle, _ptr(keys), _ptr(items), keys.numel(),
+                                                                stream))
+
+    def histogram_dev(self, t, counts, dtype: str | None = None, stream: int | None = None) -> None:
+        name = dtype or _torch_dtype_name(t)
+        check(self.lib.hpcs_histogram_byte_components_dev(self.handle, DTYPES[name], _ptr(t), t.numel(),
+                                                          _ptr(counts), stream))
+
+
+def _torch_dtype_name(t) -> str:
+    import torch
+
+    m = {torch.int32: "i32", torch.float32: "f32", torch.int64: "i64", torch.float64: "f64"}
+    if hasattr(torch, "uint32"):
+        m[torch.uint32] = "u32"
+    if hasattr(torch, "uint64"):
+        m[torch.uint64] = "u64"
+    if t.dtype not in m:
+        raise TypeError(f"unsupported tensor dtype {t.dtype}; pass dtype=")
+    return m[t.dtype]
+
+
+_default_ctx: Context | None = None
+
+
+def default_context() -> Context:
+    """Per-process context on device 0, created on first use."""
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx

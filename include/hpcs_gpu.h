@@ -1,0 +1,177 @@
+/*
+ * hpcs_gpu.h - C ABI of the B200 (sm_100a) LSD radix-sort library (libhpcs_gpu.so).
+ *
+ * This is the drop-in boundary for HPCsharp's radix-sort hot path.  A .NET caller binds
+ * these functions with P/Invoke behind the same extension methods
+ * the reference exposes; every entry point below names the reference method it replaces
+ * (paths relative to the HPCsharp project root).
+ *
+ * Conventions
+ *   - Every function returns an hpcs_status; nothing aborts, exits or traps.  The text of
+ *     the last error on the calling thread is returned by hpcs_last_error_message().
+ *   - NULL array          -> HPCS_ERR_NULL  (reference: ArgumentNullException,
+ *                                            e.g. RadixSortLsd.cs:215-216)
+ *   - bad length / k / l,r -> HPCS_ERR_RANGE (reference: ArgumentOutOfRangeException,
+ *                                            SelectionTopKRadix.cs:146-149, :164-167)
+ *   - n == 0 returns HPCS_OK at once (RadixSortLsdParallel.cs:175-176).
+ *   - One call sorts at most HPCS_MAX_KEYS keys.
+ *   - Host-array functions (no suffix) are synchronous: they copy the caller's array to
+ *     the GPU, sort, copy back into the same array and return.  The result is the
+ *     reference's in-place result (the caller's array sorted, RadixSortLsdParallel.cs:227-231).
+ *   - *_dev functions take device pointers and a cudaStream_t (passed as void*, NULL = the
+ *     context's own stream); they are asynchronous on that stream.  Device-side failures
+ *     (bounded waits that ran out) are reported by the next hpcs_ctx_synchronize().
+ *   - A context is used by one host thread at a time.  Its scratch memory is reused
+ *     across calls in stream order.
+ *   - Sorting is stable and ascending.  Signed keys order by value; float keys order by
+ *     the reference's bit transform (Histogram.cs:1210-1288): -NaN < -inf < ... < -0.0 <
+ *     +0.0 < ... < +inf < +NaN.
+ */
+#ifndef HPCS_GPU_H
+#define HPCS_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HPCS_ABI_VERSION 1
+#define HPCS_MAX_KEYS ((int64_t)1073741823) /* 2^30 - 1 keys per call */
+
+typedef enum hpcs_status {
+  HPCS_OK = 0,
+  HPCS_ERR_NULL = 1,           /* ArgumentNullException */
+  HPCS_ERR_RANGE = 2,          /* ArgumentOutOfRangeException */
+  HPCS_ERR_OOM = 3,            /* device memory or the context's pool budget exhausted */
+  HPCS_ERR_CUDA = 4,           /* a CUDA runtime call failed */
+  HPCS_ERR_DEVICE_TIMEOUT = 5, /* a bounded device-side wait ran out */
+  HPCS_ERR_UNSUPPORTED = 6,    /* dtype / option not supported */
+  HPCS_ERR_NO_DEVICE = 7,      /* no CUDA device */
+  HPCS_ERR_BUSY = 8            /* serving: admission refused */
+} hpcs_status;
+
+typedef enum hpcs_dtype {
+  HPCS_U32 = 0,
+  HPCS_I32 = 1,
+  HPCS_F32 = 2,
+  HPCS_U64 = 3,
+  HPCS_I64 = 4,
+  HPCS_F64 = 5
+} hpcs_dtype;
+
+typedef struct hpcs_ctx hpcs_ctx;
+
+typedef struct hpcs_config {
+  int64_t pool_bytes;          /* device scratch budget of the context; 0 = unlimited */
+  int32_t skip_trivial_passes; /* 1: skip a digit pass whose keys all share that digit */
+  int32_t reserved0;
+  int64_t spin_limit_ns;       /* bound on every device-side wait (default 2e9) */
+  int32_t poison_tile;         /* test hook: tile that never publishes (-1 = off) */
+  int32_t reserved[7];
+} hpcs_config;
+
+/* ---- context ---------------------------------------------------------------------- */
+void hpcs_config_default(hpcs_config* cfg);
+int hpcs_ctx_create(int device, const hpcs_config* cfg, hpcs_ctx** out);
+int hpcs_ctx_destroy(hpcs_ctx* ctx);
+/* Wait for all work of the context; reports device-side timeouts of earlier *_dev calls. */
+int hpcs_ctx_synchronize(hpcs_ctx* ctx);
+/* The context's own stream (a cudaStream_t). */
+void* hpcs_ctx_stream(hpcs_ctx* ctx);
+const char* hpcs_last_error_message(void);
+const char* hpcs_status_string(int status);
+int hpcs_abi_version(void);
+
+/* ---- per-kernel timing (tracing) ----------------------------------------------------
+ * When enabled, the context records a CUDA event pair around every kernel it launches
+ * (on the launching stream).  hpcs_ctx_profile_read waits for the context, sums the
+ * durations per kernel class and clears the record.  No reference counterpart (the
+ * reference has commented-out Stopwatch blocks in its hot loops, RadixSortLsd.cs:146-153). */
+typedef enum hpcs_kernel_class {
+  HPCS_K_HISTOGRAM = 0, /* fused all-digit histogram (+ plan) */
+  HPCS_K_ONESWEEP = 1,  /* one 8-bit digit pass */
+  HPCS_K_FINALIZE = 2,  /* copy-back / error fold */
+  HPCS_K_TOPK = 3,      /* radix select kernels */
+  HPCS_K_SEGMENTED = 4, /* batched segmented sort kernels */
+  HPCS_K_CLASSES = 8
+} hpcs_kernel_class;
+
+typedef struct hpcs_profile {
+  int64_t launches[HPCS_K_CLASSES];
+  double total_ms[HPCS_K_CLASSES];
+} hpcs_profile;
+
+int hpcs_ctx_profile_enable(hpcs_ctx* ctx, int enable);
+int hpcs_ctx_profile_read(hpcs_ctx* ctx, hpcs_profile* out);
+
+/* ---- plain sort, host arrays, in place ----------------------------------------------
+ * u32: ParallelAlgorithm.SortRadixPar(this uint[], int ParallelWorkQuantum)
+ *        RadixSortLsdParallel.cs:145-232; Algorithm.SortRadixLsd(this uint[])
+ *        RadixSortLsd.cs:255-260 (and SortRadixLsdFunc :238-243).  The work quantum is a
+ *        CPU tuning knob with no meaning on the GPU.
+ * i32: SortRadixPar(this int[]) RadixSortLsdParallel.cs:446-495; SortRadixLsd(this int[])
+ *        RadixSortLsd.cs:352-357.
+ * u64: SortRadixPar(this ulong[]) RadixSortLsdParallel.cs:690-734; SortRadixLsd(this
+ *        ulong[]) RadixSortLsd.cs:437-442.
+ * i64: SortRadixPar(this long[]) RadixSortLsdParallel.cs:560-609; SortRadixLsd(this
+ *        long[]) RadixSortLsd.cs:527-532.
+ * f32/f64: no LSD counterpart in the reference (its float radix sort is the unstable MSD
+ *        SortRadixMsd(this float[]/double[]) RadixSortMsd.cs:1563-1610); the order is the
+ *        reference's float transform, Histogram.cs:1210-1288. */
+int hpcs_sort_u32(hpcs_ctx* ctx, uint32_t* keys, int64_t n);
+int hpcs_sort_i32(hpcs_ctx* ctx, int32_t* keys, int64_t n);
+int hpcs_sort_f32(hpcs_ctx* ctx, float* keys, int64_t n);
+int hpcs_sort_u64(hpcs_ctx* ctx, uint64_t* keys, int64_t n);
+int hpcs_sort_i64(hpcs_ctx* ctx, int64_t* keys, int64_t n);
+int hpcs_sort_f64(hpcs_ctx* ctx, double* keys, int64_t n);
+
+/* ---- plain sort, device pointers, asynchronous on `stream` -------------------------- */
+int hpcs_sort_u32_dev(hpcs_ctx* ctx, uint32_t* keys, int64_t n, void* stream);
+int hpcs_sort_i32_dev(hpcs_ctx* ctx, int32_t* keys, int64_t n, void* stream);
+int hpcs_sort_f32_dev(hpcs_ctx* ctx, float* keys, int64_t n, void* stream);
+int hpcs_sort_u64_dev(hpcs_ctx* ctx, uint64_t* keys, int64_t n, void* stream);
+int hpcs_sort_i64_dev(hpcs_ctx* ctx, int64_t* keys, int64_t n, void* stream);
+int hpcs_sort_f64_dev(hpcs_ctx* ctx, double* keys, int64_t n, void* stream);
+
+/* ---- stable key + item pairs --------------------------------------------------------
+ * Algorithm.SortRadix<T>(this T[] items, UInt32[] keys) RadixSortLsd.cs:1183-1237 and
+ * SortRadix<T>(this T[] items, UInt64[] keys) :1245-1299, with T a 4-byte item (index).
+ * Both arrays are permuted in place by the stable order of the keys.  (The reference's
+ * returned Tuple.Item2 is its scratch buffer; the caller's key array is the sorted one.)
+ * i32/f32/i64/f64 keys extend the same form with the signed / float transforms. */
+int hpcs_sort_pairs_u32(hpcs_ctx* ctx, uint32_t* keys, uint32_t* items, int64_t n);
+int hpcs_sort_pairs_i32(hpcs_ctx* ctx, int32_t* keys, uint32_t* items, int64_t n);
+int hpcs_sort_pairs_f32(hpcs_ctx* ctx, float* keys, uint32_t* items, int64_t n);
+int hpcs_sort_pairs_u64(hpcs_ctx* ctx, uint64_t* keys, uint32_t* items, int64_t n);
+int hpcs_sort_pairs_i64(hpcs_ctx* ctx, int64_t* keys, uint32_t* items, int64_t n);
+int hpcs_sort_pairs_f64(hpcs_ctx* ctx, double* keys, uint32_t* items, int64_t n);
+int hpcs_sort_pairs_u32_dev(hpcs_ctx* ctx, uint32_t* keys, uint32_t* items, int64_t n, void* stream);
+int hpcs_sort_pairs_i32_dev(hpcs_ctx* ctx, int32_t* keys, uint32_t* items, int64_t n, void* stream);
+int hpcs_sort_pairs_f32_dev(hpcs_ctx* ctx, float* keys, uint32_t* items, int64_t n, void* stream);
+int hpcs_sort_pairs_u64_dev(hpcs_ctx* ctx, uint64_t* keys, uint32_t* items, int64_t n, void* stream);
+int hpcs_sort_pairs_i64_dev(hpcs_ctx* ctx, int64_t* keys, uint32_t* items, int64_t n, void* stream);
+int hpcs_sort_pairs_f64_dev(hpcs_ctx* ctx, double* keys, uint32_t* items, int64_t n, void* stream);
+
+/* ---- fused all-digit byte histogram -------------------------------------------------
+ * ParallelAlgorithm.HistogramByteComponentsPar(uint[]/int[]/ulong[]/long[], int l, int r)
+ * HistogramParallel.cs:214-222 (u32), :416-424 (i32), :547-555 (u64), :617-625 (i64), and
+ * the serial Algorithm.HistogramByteComponents Histogram.cs:261-296, :957-1052.
+ * Counts keys a[l..r] (inclusive, as the reference) into counts[P][256], P = key bytes,
+ * digit d = byte d; signed keys flip the top byte (Histogram.cs:1014, :1049), float keys
+ * use the float transform.  l > r yields all-zero counts. */
+int hpcs_histogram_byte_components_u32(hpcs_ctx* ctx, const uint32_t* a, int64_t l, int64_t r, uint32_t* counts);
+int hpcs_histogram_byte_components_i32(hpcs_ctx* ctx, const int32_t* a, int64_t l, int64_t r, uint32_t* counts);
+int hpcs_histogram_byte_components_f32(hpcs_ctx* ctx, const float* a, int64_t l, int64_t r, uint32_t* counts);
+int hpcs_histogram_byte_components_u64(hpcs_ctx* ctx, const uint64_t* a, int64_t l, int64_t r, uint32_t* counts);
+int hpcs_histogram_byte_components_i64(hpcs_ctx* ctx, const int64_t* a, int64_t l, int64_t r, uint32_t* counts);
+int hpcs_histogram_byte_components_f64(hpcs_ctx* ctx, const double* a, int64_t l, int64_t r, uint32_t* counts);
+/* Device form: a is a device pointer to the n keys, counts a device buffer of P*256. */
+int hpcs_histogram_byte_components_dev(hpcs_ctx* ctx, int dtype, const void* a, int64_t n, uint32_t* counts,
+                                       void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPCS_GPU_H */

@@ -1,0 +1,210 @@
+"""GPU parity of the plain LSD sort against the oracle (bit-exact), through the C ABI.
+
+Sizes straddle the 4096/8192-key tile boundaries and the 16-byte bulk-copy tail; the
+distributions include the adversarial ones (constant, presorted, reversed, single-bin
+digits, AND-of-3 low entropy, heavy duplicates) and the float specials."""
+import numpy as np
+import pytest
+
+from hpcsharp_b200 import algorithm, datagen, native
+from tests.gpu_util import from_dev, to_dev
+
+pytestmark = pytest.mark.gpu
+
+DTYPES = ["u32", "i32", "f32", "u64", "i64", "f64"]
+SIZES = [1, 2, 3, 5, 17, 255, 256, 257, 4095, 4096, 4097, 8191, 8192, 8193, 65539, 1_000_003]
+
+
+def oracle_sorted(orc, a):
+    s = a.copy()
+    orc.sort_radix_lsd(s)
+    return s
+
+
+def assert_same_bits(x, y):
+    assert x.dtype == y.dtype and x.shape == y.shape
+    if not np.array_equal(x.view(np.uint8), y.view(np.uint8)):
+        bad = np.flatnonzero(x.view(SIGNED_U[x.dtype.itemsize]) != y.view(SIGNED_U[y.dtype.itemsize]))
+        raise AssertionError(f"{bad.size} mismatches, first at {bad[:5]}")
+
+
+SIGNED_U = {4: np.uint32, 8: np.uint64}
+
+
+@pytest.mark.parametrize("n", SIZES)
+@pytest.mark.parametrize("dt", DTYPES)
+def test_host_sort_parity(ctx, orc, dt, n):
+    a = datagen.by_name(dt, n, seed=1000 + n)
+    want = oracle_sorted(orc, a)
+    got = a.copy()
+    ctx.sort(got)
+    assert_same_bits(got, want)
+
+
+def test_known_answer_program_cs(ctx):
+    # HPCsharpExamples/HPCsharpExamples/Program.cs:15-34
+    for dt in (np.uint32, np.int32, np.uint64, np.int64, np.float32, np.float64):
+        a = np.array([21, 43, 16, 5, 54, 3], dtype=dt)
+        ctx.sort(a)
+        assert a.tolist() == [3, 5, 16, 21, 43, 54]
+
+
+@pytest.mark.parametrize("seedfn", ["pcg32", "xorshift64s"])
+def test_config1_10m_u32(ctx, orc, seedfn):
+    """10,000,000 uint32 uniform from a seeded PCG32 / xorshift64* stream: equal to the
+    restated SortRadix (serial and parallel) and to std::sort (the Array.Sort stand-in)."""
+    n = 10_000_000
+    a = datagen.u32_pcg32_stream(n, 1) if seedfn == "pcg32" else datagen.u32_xorshift64s(n, 1)
+    serial = oracle_sorted(orc, a)
+    par = a.copy()
+    orc.sort_radix_par(par)
+    std = a.copy()
+    orc.std_sort(std)
+    got = a.copy()
+    algorithm.SortRadixPar(got)
+    assert_same_bits(got, serial)
+    assert_same_bits(got, par)
+    assert_same_bits(got, std)
+
+
+def _adversarial(dt, n, kind):
+    npdt = native.NP_OF[dt]
+    w = np.dtype(npdt).itemsize
+    u = np.uint32 if w == 4 else np.uint64
+    if kind == "constant":
+        return np.full(n, 7, dtype=u).view(npdt)
+    if kind == "zeros":
+        return np.zeros(n, dtype=npdt)
+    base = datagen.by_name(dt, n, seed=77)
+    if kind == "sorted":
+        s = base.copy()
+        s.sort(kind="stable")
+        return s
+    if kind == "reversed":
+        s = base.copy()
+        s.sort(kind="stable")
+        return s[::-1].copy()
+    if kind == "single_bin_byte1":
+        b = base.view(u).copy()
+        b &= ~u(0xFF00)
+        b |= u(0x3400)
+        return b.view(npdt)
+    if kind == "two_values":
+        b = (base.view(u) & u(1)).astype(u) * u(0x01000001)
+        return b.view(npdt)
+    if kind == "dups_mod_1000":
+        return (base.view(u) % u(1000)).astype(u).view(npdt)
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("kind", ["constant", "zeros", "sorted", "reversed", "single_bin_byte1", "two_values",
+                                  "dups_mod_1000"])
+@pytest.mark.parametrize("dt", ["u32", "i32", "f32", "u64"])
+def test_adversarial_distributions(ctx, orc, dt, kind):
+    a = _adversarial(dt, 300_001, kind)
+    want = oracle_sorted(orc, a)
+    got = a.copy()
+    ctx.sort(got)
+    assert_same_bits(got, want)
+
+
+def test_low_entropy_u64_and3(ctx, orc):
+    a = datagen.u64_and3(2_000_003, seed=3)
+    want = oracle_sorted(orc, a)
+    got = a.copy()
+    ctx.sort(got)
+    assert_same_bits(got, want)
+
+
+@pytest.mark.parametrize("skip", [True, False])
+def test_skip_trivial_passes_same_result(orc, skip):
+    c = native.Context(0, skip_trivial_passes=skip)
+    try:
+        for kind in ("single_bin_byte1", "constant", "two_values"):
+            a = _adversarial("u32", 123_457, kind)
+            want = oracle_sorted(orc, a)
+            got = a.copy()
+            c.sort(got)
+            assert_same_bits(got, want)
+    finally:
+        c.close()
+
+
+@pytest.mark.parametrize("offset", [0, 1, 3])
+@pytest.mark.parametrize("dt", DTYPES)
+def test_device_sort_parity(ctx, orc, dt, offset):
+    import torch
+
+    a = datagen.by_name(dt, 777_777, seed=21)
+    want = oracle_sorted(orc, a)
+    t = to_dev(a, offset)
+    ctx.sort_dev(t, dtype=dt, stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    assert_same_bits(from_dev(t, a.dtype), want)
+
+
+def test_repeated_calls_reuse_scratch(ctx, orc):
+    # shrinking and growing sizes on one context
+    for n in (5_000_000, 1000, 3_000_001, 8192, 1):
+        a = datagen.u32_uniform(n, seed=n)
+        want = oracle_sorted(orc, a)
+        got = a.copy()
+        ctx.sort(got)
+        assert_same_bits(got, want)
+
+
+def test_argument_errors(ctx):
+    lib = native.load()
+    a = np.zeros(10, dtype=np.uint32)
+    assert lib.hpcs_sort_u32(ctx.handle, None, 10) == native.HPCS_ERR_NULL
+    assert lib.hpcs_sort_u32(ctx.handle, a.ctypes.data, -1) == native.HPCS_ERR_RANGE
+    assert lib.hpcs_sort_u32(ctx.handle, a.ctypes.data, 0) == native.HPCS_OK
+    assert lib.hpcs_sort_u32(ctx.handle, a.ctypes.data, (1 << 30)) == native.HPCS_ERR_RANGE
+    with pytest.raises(native.ArgumentNullException):
+        algorithm.SortRadixPar(None)
+
+
+def test_subrange_sort_in_place(ctx, orc):
+    a = datagen.u32_uniform(100_000, seed=4)
+    b = a.copy()
+    algorithm.SortRadixLsd(b, 1000, 50_000)
+    want = a.copy()
+    want[1000:51_000] = oracle_sorted(orc, a[1000:51_000].copy())
+    assert_same_bits(b, want)
+
+
+def test_pool_budget_is_enforced(orc):
+    c = native.Context(0, pool_bytes=1 << 20)
+    try:
+        a = datagen.u32_uniform(1_000_000, seed=1)
+        with pytest.raises(native.HpcsError) as e:
+            c.sort(a)
+        assert e.value.status == native.HPCS_ERR_OOM
+        small = datagen.u32_uniform(10_000, seed=2)
+        want = oracle_sorted(orc, small)
+        c.sort(small)
+        assert_same_bits(small, want)
+    finally:
+        c.close()
+
+
+def test_lookback_wait_is_bounded(orc):
+    """A tile that never publishes (host-set test hook) makes every later tile's
+    look-back run out after the spin limit: the call returns HPCS_ERR_DEVICE_TIMEOUT and
+    the context stays usable."""
+    c = native.Context(0, spin_limit_ns=20_000_000, poison_tile=1)
+    try:
+        a = datagen.u32_uniform(8192 * 6, seed=1)
+        with pytest.raises(native.DeviceTimeoutError):
+            c.sort(a)
+    finally:
+        c.close()
+    c2 = native.Context(0)
+    try:
+        a = datagen.u32_uniform(8192 * 6, seed=1)
+        want = oracle_sorted(orc, a)
+        c2.sort(a)
+        assert_same_bits(a, want)
+    finally:
+        c2.close()
