@@ -366,7 +366,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                        "n": n, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (1 GiB per copy); input restored between steps"},
             "roofline": roof, "sort_roofline": sort_roof, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": launches, "clocks": clk,
+            "gpu_launches": launches, "clocks": clk, "rank_mode": ctx.rank_mode,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

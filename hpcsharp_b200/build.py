@@ -52,14 +52,18 @@ def _run(cmd: list[str]) -> None:
         sys.stderr.write(res.stderr)
 
 
-def build_gpu(force: bool = False, verbose_ptxas: bool = False) -> str:
-    out = os.path.join(PKG, "libhpcs_gpu.so")
+def build_gpu(force: bool = False, verbose_ptxas: bool = False, out: str | None = None,
+              defines: list[str] | None = None) -> str:
+    """Compile libhpcs_gpu.so; `defines` (e.g. ["HPCS_K32_KPT=12"]) build a tuning variant."""
+    out = out or os.path.join(PKG, "libhpcs_gpu.so")
     srcs = [os.path.join(CSRC, s) for s in GPU_SOURCES]
     deps = srcs + [os.path.join(CSRC, d) for d in GPU_DEPS] + [os.path.join(ROOT, "include", "hpcs_gpu.h")]
     if force or _stale(out, deps):
         flags = list(NVCC_FLAGS)
         if verbose_ptxas:
             flags += ["-Xptxas", "-v"]
+        for d in defines or []:
+            flags += ["-D" + d]
         _run([_nvcc(), *flags, "-o", out, *srcs])
     return out
 

@@ -108,6 +108,30 @@ cudaStream_t pick_stream(hpcs_ctx* ctx, void* stream) {
   return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
 }
 
+// Runs the lane-order probe once per device (result cached per device).
+int probe_rank_order(hpcs_ctx* ctx, int* ordered) {
+  static std::mutex mu;
+  static int cache[64];  // 0 unknown, 1 ordered, 2 not ordered
+  std::lock_guard<std::mutex> lock(mu);
+  int& c = cache[ctx->device & 63];
+  if (c == 0) {
+    uint32_t* bad = nullptr;
+    HPCS_CUDA(cudaMalloc(&bad, 4));
+    cudaError_t e = cudaMemset(bad, 0, 4);
+    if (e == cudaSuccess) {
+      rank_probe_kernel<512, 16><<<ctx->sms * 2, 512>>>(bad, 0x2545F491u);
+      e = cudaGetLastError();
+    }
+    uint32_t h = 1;
+    if (e == cudaSuccess) e = cudaMemcpy(&h, bad, 4, cudaMemcpyDeviceToHost);
+    cudaFree(bad);
+    if (e != cudaSuccess) return cuda_fail(e, "rank order probe");
+    c = h == 0 ? 1 : 2;
+  }
+  *ordered = c == 1;
+  return HPCS_OK;
+}
+
 // Reads and clears the accumulated device error bits (synchronous).
 int check_device_errors(hpcs_ctx* ctx) {
   uint32_t bits = 0;
@@ -204,17 +228,9 @@ int enqueue_histogram(hpcs_ctx* ctx, const U* d, int64_t n, uint32_t* counts, cu
     HPCS_CUDA(cudaMemcpyAsync(ctx->keys_b.ptr, d, size_t(n) * sizeof(U), cudaMemcpyDeviceToDevice, s));
     src = static_cast<const U*>(ctx->keys_b.ptr);
   }
-  auto k = hist_all_digits_kernel<U, KIND, HIST_NT>;
-  static int blocks = 0;
-  if (!blocks) blocks = occupancy_blocks(k, HIST_NT, 0);
-  const int64_t vec = n * int64_t(sizeof(U)) / 16;
-  int64_t want = (vec + HIST_NT * 4 - 1) / (HIST_NT * 4);
-  int64_t cap = int64_t(ctx->sms) * blocks;
-  int grid = int(want < 1 ? 1 : (want > cap ? cap : want));
   SortArgs none{};
-  k<<<grid, HIST_NT, 0, s>>>(src, n, counts, none, 0);
-  HPCS_CUDA(cudaGetLastError());
-  return HPCS_OK;
+  KernelTimer kt(ctx, s, HPCS_K_HISTOGRAM);
+  return launch_histogram<U, KIND>(ctx, src, n, counts, none, 0, s);
 }
 
 template <class T, class U, int KIND>
@@ -259,6 +275,7 @@ void hpcs_config_default(hpcs_config* cfg) {
   cfg->skip_trivial_passes = 1;
   cfg->spin_limit_ns = 2000000000LL;
   cfg->poison_tile = -1;
+  cfg->rank_mode = 0;
 }
 
 int hpcs_abi_version(void) { return HPCS_ABI_VERSION; }
@@ -315,6 +332,15 @@ int hpcs_ctx_create(int device, const hpcs_config* cfg, hpcs_ctx** out) {
   if (rc != HPCS_OK || cudaMemset(ctx->err_accum.ptr, 0, 256) != cudaSuccess) {
     hpcs_ctx_destroy(ctx);
     return rc != HPCS_OK ? rc : fail(HPCS_ERR_CUDA, "cudaMemset");
+  }
+  ctx->rank_mode = RANK_PEER_MASK;
+  if (ctx->cfg.rank_mode == 0) {
+    int ordered = 0;
+    if ((rc = probe_rank_order(ctx, &ordered)) != HPCS_OK) {
+      hpcs_ctx_destroy(ctx);
+      return rc;
+    }
+    if (ordered) ctx->rank_mode = RANK_ORDERED_ATOMIC;
   }
   *out = ctx;
   return HPCS_OK;
@@ -374,6 +400,17 @@ int hpcs_ctx_profile_read(hpcs_ctx* ctx, hpcs_profile* out) {
 }
 
 void* hpcs_ctx_stream(hpcs_ctx* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+int hpcs_ctx_trace_tiles(hpcs_ctx* ctx, uint64_t* trace, int capacity_tiles, int pass) {
+  if (!ctx) return fail(HPCS_ERR_NULL, "ctx is NULL");
+  if (trace && capacity_tiles <= 0) return fail(HPCS_ERR_RANGE, "capacity must be positive");
+  ctx->trace = trace;
+  ctx->trace_capacity = trace ? capacity_tiles : 0;
+  ctx->trace_pass = pass;
+  return HPCS_OK;
+}
+
+int hpcs_ctx_rank_mode(hpcs_ctx* ctx) { return ctx ? ctx->rank_mode : -HPCS_ERR_NULL; }
 
 // ---- plain sorts ----
 int hpcs_sort_u32(hpcs_ctx* c, uint32_t* k, int64_t n) { return sort_host<uint32_t, uint32_t, KIND_UNSIGNED>(c, k, n); }

@@ -25,6 +25,8 @@
 #include <cstdint>
 #include <type_traits>
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace hpcs {
@@ -38,6 +40,11 @@ constexpr uint32_t ST_PREFIX = 2u << 30;     // inclusive prefix over tiles 0..t
 constexpr uint32_t ST_FLAGS = 3u << 30;
 constexpr uint32_t ST_VALUE = (1u << 30) - 1;
 constexpr int64_t MAX_KEYS_PER_SORT = (int64_t(1) << 30) - 1;
+// Predecessor status words read per look-back step.
+#ifndef HPCS_LB_WINDOW
+#define HPCS_LB_WINDOW 8
+#endif
+constexpr int LB_WINDOW = HPCS_LB_WINDOW;
 
 struct NoValue {};
 
@@ -67,75 +74,97 @@ struct SortArgs {
   int skip_trivial;
   int poison_tile;        // test hook: this tile never publishes (-1 = off)
   uint64_t spin_limit_ns; // bound on every device-side wait
+  // Tile trace (debug): when non-null, thread 0 writes TRACE_WORDS stamps per tile of
+  // pass `trace_pass`: tile id, SM id, then %globaltimer at start, data ready, ranked,
+  // look-back done (digit 0), end of scatter.
+  uint64_t* trace;
+  int trace_pass;
+  int trace_capacity;  // tiles
 };
+constexpr int TRACE_WORDS = 7;
+
+__device__ __forceinline__ uint32_t sm_id() {
+  uint32_t v;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(v));
+  return v;
+}
 
 // =====================================================================================
 // K1: fused all-digit histogram (+ plan in the last CTA)
 // =====================================================================================
+// Counters are privatised per lane: bin b of digit d for lane l lives at word
+// (d*256 + b)*COPIES + l % COPIES, so the 32 shared atomics of one warp instruction fall in
+// (nearly) distinct banks whatever the key values -- one shared-memory wavefront each
+// instead of ~3.3 for random bins.  32-bit keys: 32 copies (4 x 256 x 32 words = 128 KiB);
+// 64-bit keys: 16 copies (8 x 256 x 16 words = 128 KiB).
+template <class U>
+struct HistSmem {
+  static constexpr int P = int(sizeof(U));
+  static constexpr int COPIES = P == 4 ? 32 : 16;
+  static constexpr size_t BYTES = size_t(P) * RADIX * COPIES * 4;
+};
+
 template <class U, int KIND, int NT>
-__global__ void __launch_bounds__(NT) hist_all_digits_kernel(const U* __restrict__ keys, int64_t n,
-                                                              uint32_t* __restrict__ hist_out,
-                                                              SortArgs args, int make_plan) {
-  constexpr int P = int(sizeof(U));
+__global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restrict__ keys, int64_t n,
+                                                                 uint32_t* __restrict__ hist_out,
+                                                                 SortArgs args, int make_plan) {
+  constexpr int P = HistSmem<U>::P;
+  constexpr int COPIES = HistSmem<U>::COPIES;
   constexpr int VEC = 16 / int(sizeof(U));
   using KO = KeyOrder<U, KIND>;
-  __shared__ uint32_t sh[P][RADIX];
+  extern __shared__ __align__(16) uint32_t sh[];  // [P][256][COPIES]
   __shared__ uint32_t s_last;
   const int tid = threadIdx.x;
-  for (int i = tid; i < P * RADIX; i += NT) (&sh[0][0])[i] = 0;
+  const int lane = tid & 31;
+  const int copy = lane & (COPIES - 1);
+  for (int i = tid; i < P * RADIX * COPIES; i += NT) sh[i] = 0;
   __syncthreads();
 
-  // Count the P digits of one key.  Every lane of the warp calls this together (the loop
-  // bounds below are warp-uniform); lanes without a key pass valid = false.
-  auto count_key = [&](U k, bool valid) {
-    U o = KO::to_ordered(k);
+  auto count_key = [&](U k) {
+    const U o = KO::to_ordered(k);
 #pragma unroll
     for (int d = 0; d < P; d++) {
-      uint32_t dg = uint32_t(o >> (8 * d)) & 0xFFu;
-      // Lane 0 holds a key whenever any lane does (indices grow with the lane).
-      uint32_t first = __shfl_sync(0xFFFFFFFFu, dg, 0);
-      if (__all_sync(0xFFFFFFFFu, !valid || dg == first)) {
-        // constant or heavily skewed byte: one atomic for the warp
-        uint32_t cnt = __popc(__ballot_sync(0xFFFFFFFFu, valid));
-        if ((tid & 31) == 0 && cnt) atomicAdd(&sh[d][first], cnt);
-      } else if (valid) {
-        atomicAdd(&sh[d][dg], 1u);
-      }
+      const uint32_t dg = uint32_t(o >> (8 * d)) & 0xFFu;
+      atomicAdd(&sh[(d * RADIX + dg) * COPIES + copy], 1u);
     }
   };
 
   const int64_t nvec = n / VEC;
   const uint4* vkeys = reinterpret_cast<const uint4*>(keys);
   const int64_t stride = int64_t(gridDim.x) * NT;
-  const int lane = tid & 31;
-  // Warp-uniform grid-stride loop, 4 vectors in flight per thread per iteration.
-  for (int64_t wb = int64_t(blockIdx.x) * NT + (tid - lane); wb < nvec; wb += 4 * stride) {
+  int64_t i = int64_t(blockIdx.x) * NT + tid;
+  // 4 vectors in flight per thread per iteration
+  for (; i + 3 * stride < nvec; i += 4 * stride) {
     uint4 v[4];
-    bool ok[4];
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const int64_t idx = wb + lane + int64_t(u) * stride;
-      ok[u] = idx < nvec;
-      v[u] = ok[u] ? ldg_stream_v4(vkeys + idx) : make_uint4(0, 0, 0, 0);
-    }
+    for (int u = 0; u < 4; u++) v[u] = ldg_stream_v4(vkeys + i + u * stride);
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       const U* e = reinterpret_cast<const U*>(&v[u]);
 #pragma unroll
-      for (int j = 0; j < VEC; j++) count_key(e[j], ok[u]);
+      for (int j = 0; j < VEC; j++) count_key(e[j]);
     }
   }
-  // Ragged tail (fewer than VEC keys): warp 0 of block 0.
-  if (blockIdx.x == 0 && tid < 32) {
+  for (; i < nvec; i += stride) {
+    const uint4 v = ldg_stream_v4(vkeys + i);
+    const U* e = reinterpret_cast<const U*>(&v);
+#pragma unroll
+    for (int j = 0; j < VEC; j++) count_key(e[j]);
+  }
+  // ragged tail (fewer than VEC keys)
+  if (blockIdx.x == 0 && tid < VEC) {
     const int64_t t = nvec * VEC + tid;
-    const bool valid = t < n;
-    count_key(valid ? keys[t] : U(0), valid);
+    if (t < n) count_key(keys[t]);
   }
   __syncthreads();
+  // fold the copies (rotated start so a warp's reads hit distinct banks) into the output
   for (int j = tid; j < P * RADIX; j += NT) {
-    uint32_t c = (&sh[0][0])[j];
+    uint32_t c = 0;
+#pragma unroll 8
+    for (int q = 0; q < COPIES; q++) c += sh[j * COPIES + ((q + lane) & (COPIES - 1))];
     if (c) atomicAdd(hist_out + j, c);
   }
+
   if (!make_plan) return;
 
   // Zero the first look-back buffer for the first executed pass, and the tile counters.
@@ -208,7 +237,46 @@ __global__ void __launch_bounds__(NT) hist_all_digits_kernel(const U* __restrict
 // =====================================================================================
 // K3: one 8-bit digit pass (onesweep)
 // =====================================================================================
-template <class U, class V, int NT, int KPT, int STAGES>
+//
+// In-warp stable ranking.  Keys sit warp-striped (key i of lane l is tile position
+// w*32*KPT + i*32 + l), so a warp's keys in (i, lane) order are in input order.  Each warp
+// owns 256 digit counters in shared memory; the rank of a key among the warp's earlier
+// keys with the same digit is
+//   RANK_ORDERED_ATOMIC  the value returned by one shared-memory atomicAdd per key.  This
+//                        relies on the hardware resolving same-address atomics of one warp
+//                        instruction in ascending lane order.  PTX leaves that order
+//                        undefined, so every context verifies it first with
+//                        rank_probe_kernel (the same code path) and otherwise uses:
+//   RANK_PEER_MASK       fully defined: each lane ORs its lane bit into a per-(warp, digit)
+//                        mask; after __syncwarp the mask is the set of same-digit lanes
+//                        (the peers), the rank is counter + popc(peers below me), and the
+//                        lowest peer advances the counter and clears the mask.
+// Both give identical ranks.  (__match_any_sync / ballots would also be defined but
+// run 10-20x slower than one shared atomic on this part.)
+enum RankMode : int { RANK_ORDERED_ATOMIC = 0, RANK_PEER_MASK = 1 };
+
+template <int MODE>
+__device__ __forceinline__ uint32_t rank_in_warp(uint32_t* cnt, uint32_t* msk, uint32_t d, bool valid, int parity,
+                                                 int lane) {
+  if (MODE == RANK_ORDERED_ATOMIC) {
+    return valid ? atomicAdd(&cnt[d], 1u) : 0u;
+  } else {
+    uint32_t* m = msk + parity * RADIX + (valid ? d : 0u);
+    if (valid) atomicOr(m, 1u << lane);
+    __syncwarp();
+    const uint32_t peers = valid ? *reinterpret_cast<volatile uint32_t*>(m) : 0u;
+    const uint32_t before = valid ? cnt[d] : 0u;
+    const uint32_t lt = peers & lanemask_lt();
+    __syncwarp();
+    if (valid && lt == 0u) {
+      cnt[d] = before + __popc(peers);
+      *m = 0u;
+    }
+    return before + __popc(lt);
+  }
+}
+
+template <class U, class V, int NT, int KPT, int STAGES, int MODE>
 struct OnesweepSmem {
   static constexpr bool PAIRS = !std::is_same<V, NoValue>::value;
   static constexpr int TILE = NT * KPT;
@@ -217,26 +285,32 @@ struct OnesweepSmem {
   static constexpr size_t VALS_BYTES = PAIRS ? size_t(TILE) * 4 : 0;
   static constexpr size_t STAGE_BYTES = KEYS_BYTES + VALS_BYTES;
   static constexpr size_t OFF_STAGES = 0;
-  static constexpr size_t OFF_WHIST = OFF_STAGES + STAGE_BYTES * STAGES;
-  static constexpr size_t OFF_BINSTART = OFF_WHIST + size_t(NW) * RADIX * 4;
-  static constexpr size_t OFF_TOTAL = OFF_BINSTART + RADIX * 4;
-  static constexpr size_t OFF_LOCAL = OFF_TOTAL + RADIX * 4;
+  static constexpr size_t OFF_CNT = OFF_STAGES + STAGE_BYTES * STAGES;      // [NW][256]
+  static constexpr size_t OFF_MSK = OFF_CNT + size_t(NW) * RADIX * 4;        // [NW][2][256]
+  static constexpr size_t MSK_BYTES = MODE == RANK_PEER_MASK ? size_t(NW) * 2 * RADIX * 4 : 0;
+  static constexpr size_t OFF_BINSTART = OFF_MSK + MSK_BYTES;
+  static constexpr size_t OFF_LOCAL = OFF_BINSTART + RADIX * 4;
   static constexpr size_t OFF_GBASE = OFF_LOCAL + RADIX * 4;
-  static constexpr size_t OFF_WSUM = OFF_GBASE + RADIX * 4;
+  static constexpr size_t OFF_TOT = OFF_GBASE + RADIX * 4;   // this CTA's digit totals
+  static constexpr size_t OFF_CPRE = OFF_TOT + RADIX * 4;    // earlier CTAs of the unit
+  static constexpr size_t OFF_EXCL = OFF_CPRE + RADIX * 4;   // unit exclusive prefix (rank 0)
+  static constexpr size_t OFF_WSUM = OFF_EXCL + RADIX * 4;
   static constexpr size_t OFF_TILE = OFF_WSUM + 32 * 4;
   static constexpr size_t OFF_MBAR = (OFF_TILE + 16 + 7) / 8 * 8;
   static constexpr size_t BYTES = OFF_MBAR + 8 * STAGES;
 };
 
-// Issue the bulk copy of tile t into stage s (called by one thread).  The 16-byte-aligned
-// body is copied by the TMA engine; the ragged tail (< 16 bytes) is read with plain loads
-// by the consumers.  Stage buffers start at offset 0 of the dynamic shared memory.
+// Issue the bulk copy of sub-tile `sub` into stage s (called by one thread).  The
+// 16-byte-aligned body is copied by the TMA engine; the ragged tail (< 16 bytes) is read
+// with plain loads by the consumers.  Stage buffers start at offset 0 of the dynamic
+// shared memory.  A sub-tile past the end arrives with zero bytes.
 template <class U, bool PAIRS, int TILE>
 __device__ __forceinline__ void onesweep_issue_tile(unsigned char* smem, size_t stage_bytes, size_t keys_bytes,
                                                     uint64_t* mbar, const U* kin, const uint32_t* vin,
-                                                    int64_t n, int t, int s) {
-  const int64_t base = int64_t(t) * TILE;
-  const int64_t cnt = (n - base) < TILE ? (n - base) : TILE;
+                                                    int64_t n, int64_t sub, int s) {
+  const int64_t base = sub * TILE;
+  int64_t cnt = n - base;
+  cnt = cnt < 0 ? 0 : (cnt < TILE ? cnt : TILE);
   const uint32_t kbytes = uint32_t((cnt * int64_t(sizeof(U))) & ~int64_t(15));
   const uint32_t vbytes = PAIRS ? uint32_t((cnt * 4) & ~int64_t(15)) : 0u;
   unsigned char* dst = smem + size_t(s) * stage_bytes;
@@ -246,19 +320,42 @@ __device__ __forceinline__ void onesweep_issue_tile(unsigned char* smem, size_t 
   if (PAIRS && vbytes) bulk_copy_g2s(dst + keys_bytes, vin + base, vbytes, &mbar[s]);
 }
 
-template <class U, int KIND, class V, int NT, int KPT, int STAGES, int MINB>
+// Barrier over the CTAs of a cluster (all threads), or over the CTA when CL == 1.
+template <int CL>
+__device__ __forceinline__ void unit_sync() {
+  if (CL > 1) {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+  } else {
+    __syncthreads();
+  }
+}
+
+// Address of `p` (a shared-memory location of this CTA) in the CTA of cluster rank `r`.
+template <class T>
+__device__ __forceinline__ T* cluster_peer(T* p, uint32_t r) {
+  return cooperative_groups::this_cluster().map_shared_rank(p, r);
+}
+
+// One onesweep digit pass.  The look-back unit is a cluster of CL CTAs: the CTAs of a
+// cluster each stage, rank and reorder their own TILE-key sub-tile, exchange their digit
+// totals through distributed shared memory, and cluster rank 0 publishes one aggregate and
+// runs one look-back for all CL x TILE keys.  This divides the rate at which look-back
+// units are produced by CL: a decoupled look-back advances at most LB_WINDOW units per L2
+// round trip, which otherwise caps a B200 pass well below its HBM bandwidth.
+template <class U, int KIND, class V, int NT, int KPT, int STAGES, int MINB, int MODE, int CL>
 __global__ void __launch_bounds__(NT, MINB) onesweep_pass_kernel(SortArgs args) {
-  using L = OnesweepSmem<U, V, NT, KPT, STAGES>;
+  using L = OnesweepSmem<U, V, NT, KPT, STAGES, MODE>;
   using KO = KeyOrder<U, KIND>;
   constexpr bool PAIRS = L::PAIRS;
   constexpr int TILE = L::TILE;
   constexpr int NW = L::NW;
   static_assert(NT >= RADIX && NT % 32 == 0, "one thread per digit needed");
+  static_assert(STAGES == 2, "two stages: one being processed, one being filled");
 
   const SortPlan* plan = args.plan;
   const int pass = args.pass;
   const int sel = plan->src_sel[pass];
-  if (sel < 0) return;  // every key has the same digit here: the pass is the identity
+  if (sel < 0) return;  // every key has the same digit here: the pass is the identity (uniform)
   const int shift = 8 * pass;
   const U* __restrict__ kin = static_cast<const U*>(sel ? args.keys_b : args.keys_a);
   U* __restrict__ kout = static_cast<U*>(sel ? args.keys_a : args.keys_b);
@@ -271,58 +368,81 @@ __global__ void __launch_bounds__(NT, MINB) onesweep_pass_kernel(SortArgs args) 
   uint32_t* tile_counter = const_cast<uint32_t*>(&plan->tile_counter[pass]);
   uint32_t* err = const_cast<uint32_t*>(&plan->error);
   const int64_t n = args.n;
-  const int num_tiles = args.num_tiles;
+  const int num_units = args.num_tiles;  // look-back units (clusters of CL sub-tiles)
+  const uint32_t crank = CL > 1 ? cooperative_groups::this_cluster().block_rank() : 0u;
 
   extern __shared__ __align__(128) unsigned char smem[];
-  uint32_t* s_whist = reinterpret_cast<uint32_t*>(smem + L::OFF_WHIST);  // [NW][256]
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + L::OFF_CNT);  // [NW][256]
+  uint32_t* s_msk = reinterpret_cast<uint32_t*>(smem + L::OFF_MSK);  // [NW][2][256] (peer-mask mode)
   uint32_t* s_binstart = reinterpret_cast<uint32_t*>(smem + L::OFF_BINSTART);
-  uint32_t* s_total = reinterpret_cast<uint32_t*>(smem + L::OFF_TOTAL);
   uint32_t* s_local = reinterpret_cast<uint32_t*>(smem + L::OFF_LOCAL);
   uint32_t* s_gbase = reinterpret_cast<uint32_t*>(smem + L::OFF_GBASE);
+  uint32_t* s_tot = reinterpret_cast<uint32_t*>(smem + L::OFF_TOT);
+  uint32_t* s_cpre = reinterpret_cast<uint32_t*>(smem + L::OFF_CPRE);
+  uint32_t* s_excl = reinterpret_cast<uint32_t*>(smem + L::OFF_EXCL);
   uint32_t* s_wsum = reinterpret_cast<uint32_t*>(smem + L::OFF_WSUM);
   int* s_tile = reinterpret_cast<int*>(smem + L::OFF_TILE);
   uint64_t* s_mbar = reinterpret_cast<uint64_t*>(smem + L::OFF_MBAR);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t* cnt_w = s_cnt + warp * RADIX;
+  uint32_t* msk_w = s_msk + warp * 2 * RADIX;
+
+  // Rank 0 takes the next unit and writes its id into every CTA of the cluster.
+  auto acquire_and_broadcast = [&](int slot) {
+    const int u = int(atomicAdd(tile_counter, 1u));
+    if (CL > 1) {
+      for (uint32_t q = 0; q < uint32_t(CL); q++) *cluster_peer(&s_tile[slot], q) = u;
+    } else {
+      s_tile[slot] = u;
+    }
+  };
 
   if (tid == 0) {
-    for (int s = 0; s < STAGES; s++) mbar_init(&s_mbar[s], 1);
+    for (int st = 0; st < STAGES; st++) mbar_init(&s_mbar[st], 1);
     fence_mbar_init();
     fence_proxy_async_smem();
   }
   for (int i = tid; i < RADIX; i += NT) s_binstart[i] = plan->bin_start[pass][i];
-  __syncthreads();
-  if (tid == 0) {
-    int t0 = int(atomicAdd(tile_counter, 1u));
-    s_tile[0] = t0;
-    if (t0 < num_tiles) onesweep_issue_tile<U, PAIRS, TILE>(smem, L::STAGE_BYTES, L::KEYS_BYTES, s_mbar, kin, vin, n, t0, 0);
-  }
-  __syncthreads();
+  if (MODE == RANK_PEER_MASK)
+    for (int i = lane; i < 2 * RADIX; i += 32) msk_w[i] = 0u;
+  if (CL > 1) unit_sync<CL>();  // peers' shared memory is live before remote writes
+  if (crank == 0 && tid == 0) acquire_and_broadcast(0);
+  unit_sync<CL>();
+  if (tid == 0 && s_tile[0] < num_units)
+    onesweep_issue_tile<U, PAIRS, TILE>(smem, L::STAGE_BYTES, L::KEYS_BYTES, s_mbar, kin, vin, n,
+                                        int64_t(s_tile[0]) * CL + crank, 0);
 
   uint32_t phase_bits = 0;  // bit s = parity to wait for on stage s
   int stage = 0;
   for (;;) {
-    const int t = s_tile[stage];
-    if (t >= num_tiles) break;
-    if (STAGES > 1 && tid == 0) {
-      int tn = int(atomicAdd(tile_counter, 1u));
-      s_tile[stage ^ 1] = tn;
-      if (tn < num_tiles)
-        onesweep_issue_tile<U, PAIRS, TILE>(smem, L::STAGE_BYTES, L::KEYS_BYTES, s_mbar, kin, vin, n, tn, stage ^ 1);
-    }
-    const int64_t tile_base = int64_t(t) * TILE;
-    const int tile_n = int((n - tile_base) < TILE ? (n - tile_base) : TILE);
+    const int u = s_tile[stage];  // the same in every CTA of the cluster
+    if (u >= num_units) break;
+    // next unit: taken now (one iteration ahead), issued after the first cluster barrier
+    if (crank == 0 && tid == 0) acquire_and_broadcast(stage ^ 1);
+    const int64_t tile_base = (int64_t(u) * CL + crank) * TILE;
+    int64_t tn64 = n - tile_base;
+    const int tile_n = int(tn64 < 0 ? 0 : (tn64 < TILE ? tn64 : TILE));
     const int bulk_keys = int((int64_t(tile_n) * int64_t(sizeof(U))) & ~int64_t(15)) / int(sizeof(U));
     const int bulk_vals = PAIRS ? int((int64_t(tile_n) * 4) & ~int64_t(15)) / 4 : 0;
+    uint64_t* trace = (args.trace && pass == args.trace_pass && u < args.trace_capacity && tid == 0 && crank == 0)
+                          ? args.trace + int64_t(u) * TRACE_WORDS
+                          : nullptr;
+    if (trace) {
+      trace[0] = uint64_t(u);
+      trace[1] = sm_id();
+      trace[2] = global_timer_ns();
+    }
 
     // zero this warp's digit counters
-    for (int i = lane; i < RADIX; i += 32) s_whist[warp * RADIX + i] = 0;
+    for (int i = lane; i < RADIX; i += 32) cnt_w[i] = 0u;
 
-    // wait for the staged tile (bounded)
+    // wait for the staged sub-tile (bounded)
     if (!mbar_wait_bounded(&s_mbar[stage], (phase_bits >> stage) & 1u, args.spin_limit_ns)) {
       if (lane == 0) atomicOr(err, uint32_t(DERR_TMA_TIMEOUT));
     }
     phase_bits ^= (1u << stage);
     __syncwarp();
+    if (trace) trace[3] = global_timer_ns();
 
     // ---- load keys (warp-striped) and rank them within the warp --------------------
     U* sk = reinterpret_cast<U*>(smem + L::OFF_STAGES + stage * L::STAGE_BYTES);
@@ -341,99 +461,147 @@ __global__ void __launch_bounds__(NT, MINB) onesweep_pass_kernel(SortArgs args) 
     for (int i = 0; i < KPT; i++) {
       const int idx = wbase + i * 32 + lane;
       const bool valid = idx < tile_n;
-      const uint32_t d = valid ? KO::digit(key[i], shift) : 0x100u;
-      const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-      const int leader = __ffs(peers) - 1;
-      uint32_t before = 0;
-      if (lane == leader && valid) {
-        before = s_whist[warp * RADIX + d];
-        s_whist[warp * RADIX + d] = before + __popc(peers);
-      }
-      before = __shfl_sync(0xFFFFFFFFu, before, leader);
-      rank[i] = before + __popc(peers & lanemask_lt());
-      __syncwarp();
+      rank[i] = rank_in_warp<MODE>(cnt_w, msk_w, KO::digit(key[i], shift), valid, i & 1, lane);
     }
     __syncthreads();  // (A) warp counts complete; stage buffer no longer read
+    if (trace) trace[4] = global_timer_ns();
 
-    // ---- per digit: exclusive prefix over warps, tile total, publish aggregate -----
+    // ---- per digit: sub-tile total and scan over digits -------------------------------
     if (tid < RADIX) {
       const int dg = tid;
-      uint32_t run = 0;
+      uint32_t total = 0;
 #pragma unroll
-      for (int w = 0; w < NW; w++) {
-        uint32_t c = s_whist[w * RADIX + dg];
-        s_whist[w * RADIX + dg] = run;
-        run += c;
-      }
-      s_total[dg] = run;
-      if (t != args.poison_tile) {
-        if (t == 0) st_relaxed_gpu(&status[dg], ST_PREFIX | run);
-        else st_relaxed_gpu(&status[int64_t(t) * RADIX + dg], ST_AGGREGATE | run);
-      }
-      // warp-inclusive scan of the totals (digit order)
-      uint32_t incl = run;
+      for (int w = 0; w < NW; w++) total += s_cnt[w * RADIX + dg];
+      s_tot[dg] = total;
+      uint32_t incl = total;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
         if (lane >= o) incl += y;
       }
-      s_local[dg] = incl;  // inclusive within the warp for now
+      s_local[dg] = incl - total;  // exclusive within this warp of digits for now
       if (lane == 31) s_wsum[warp] = incl;
     }
     __syncthreads();  // (B)
+    // sub-tile start of each digit; counters become (digit start + earlier warps' count)
     if (tid < RADIX) {
       const int dg = tid;
       uint32_t base = 0;
 #pragma unroll
       for (int w = 0; w < RADIX / 32; w++) base += (w < warp) ? s_wsum[w] : 0u;
-      s_local[dg] = base + s_local[dg] - s_total[dg];
+      const uint32_t local = base + s_local[dg];
+      s_local[dg] = local;
+      uint32_t run = local;
+#pragma unroll
+      for (int w = 0; w < NW; w++) {
+        const uint32_t c = s_cnt[w * RADIX + dg];
+        s_cnt[w * RADIX + dg] = run;
+        run += c;
+      }
     }
-    __syncthreads();  // (B2) tile-local digit starts ready
+    unit_sync<CL>();  // (C1) offsets ready; every CTA's totals and the next unit id visible
 
-    // ---- decoupled look-back (one thread per digit), overlapped with the reorder ----
+    // prefetch the next sub-tile into the other stage (its previous contents are done)
+    if (tid == 0) {
+      const int un = s_tile[stage ^ 1];
+      if (un < num_units)
+        onesweep_issue_tile<U, PAIRS, TILE>(smem, L::STAGE_BYTES, L::KEYS_BYTES, s_mbar, kin, vin, n,
+                                            int64_t(un) * CL + crank, stage ^ 1);
+    }
+
+    // ---- unit totals, aggregate, decoupled look-back (rank 0), overlapped with reorder ----
     if (tid < RADIX) {
       const int dg = tid;
-      uint32_t excl = 0;
-      if (t > 0) {
-        int j = t - 1;
-        uint64_t t0 = 0;
-        bool timed_out = false;
-        while (j >= 0) {
-          uint32_t s = ld_relaxed_gpu(&status[int64_t(j) * RADIX + dg]);
-          if ((s & ST_FLAGS) == 0) {
-            if (t0 == 0) t0 = global_timer_ns();
-            else if (global_timer_ns() - t0 > args.spin_limit_ns || ld_volatile(err) != 0u) {
-              timed_out = true;
-              break;
-            }
-            continue;
-          }
-          t0 = 0;
-          excl += s & ST_VALUE;
-          if (s & ST_PREFIX) break;
-          j--;
+      uint32_t utot = 0, cpre = 0;
+      if (CL > 1) {
+#pragma unroll
+        for (int q = 0; q < CL; q++) {
+          const uint32_t v = *cluster_peer(&s_tot[dg], uint32_t(q));
+          utot += v;
+          cpre += (uint32_t(q) < crank) ? v : 0u;
         }
-        if (timed_out) atomicOr(err, uint32_t(DERR_LOOKBACK_TIMEOUT));
-        if (t != args.poison_tile)
-          st_relaxed_gpu(&status[int64_t(t) * RADIX + dg], ST_PREFIX | ((excl + s_total[dg]) & ST_VALUE));
+      } else {
+        utot = s_tot[dg];
       }
-      s_gbase[dg] = s_binstart[dg] + excl - s_local[dg];
-      // zero-ahead: clear this tile's words in the buffer the next executed pass uses
-      status_next[int64_t(t) * RADIX + dg] = 0;
+      s_cpre[dg] = cpre;
+      if (crank == 0) {
+        if (u != args.poison_tile) {
+          if (u == 0) st_relaxed_gpu(&status[dg], ST_PREFIX | utot);
+          else st_relaxed_gpu(&status[int64_t(u) * RADIX + dg], ST_AGGREGATE | utot);
+        }
+        uint32_t excl = 0;
+        if (u > 0) {
+          // Windowed walk: read LB_WINDOW predecessors' words at once (independent
+          // loads), sum the ready ones from the nearest outward and stop at the first
+          // inclusive prefix.
+          int j = u - 1;
+          uint64_t t0 = 0;
+          bool timed_out = false;
+          while (true) {
+            uint32_t wv[LB_WINDOW];
+#pragma unroll
+            for (int q = 0; q < LB_WINDOW; q++)
+              wv[q] = (j - q >= 0) ? ld_relaxed_gpu(&status[int64_t(j - q) * RADIX + dg]) : (ST_PREFIX | 0u);
+            int used = 0;
+            bool found = false;
+#pragma unroll
+            for (int q = 0; q < LB_WINDOW; q++) {
+              if (used == q) {  // still contiguous from the nearest predecessor
+                const uint32_t v = wv[q];
+                if ((v & ST_FLAGS) != 0) {
+                  excl += v & ST_VALUE;
+                  used = q + 1;
+                  if (v & ST_PREFIX) found = true;
+                }
+              }
+              if (found) break;
+            }
+            if (found) break;
+            j -= used;
+            if (used == 0) {
+              // nearest predecessor not published yet: spin on that one word with a short
+              // back-off (frees issue slots for the reordering warps), bounded in time
+              uint32_t v;
+              while (((v = ld_relaxed_gpu(&status[int64_t(j) * RADIX + dg])) & ST_FLAGS) == 0) {
+                __nanosleep(32);
+                if (t0 == 0) t0 = global_timer_ns();
+                else if (global_timer_ns() - t0 > args.spin_limit_ns || ld_volatile(err) != 0u) {
+                  timed_out = true;
+                  break;
+                }
+              }
+              if (timed_out) break;
+            }
+          }
+          if (timed_out) atomicOr(err, uint32_t(DERR_LOOKBACK_TIMEOUT));
+          if (u != args.poison_tile)
+            st_relaxed_gpu(&status[int64_t(u) * RADIX + dg], ST_PREFIX | ((excl + utot) & ST_VALUE));
+        }
+        s_excl[dg] = excl;
+        // zero-ahead: clear this unit's words in the buffer the next executed pass uses
+        status_next[int64_t(u) * RADIX + dg] = 0;
+        if (trace) trace[5] = global_timer_ns();
+      }
     }
 
-    // ---- reorder the tile in shared memory by digit -----------------------------------
+    // ---- reorder the sub-tile in shared memory by digit -------------------------------
 #pragma unroll
     for (int i = 0; i < KPT; i++) {
       const int idx = wbase + i * 32 + lane;
       if (idx < tile_n) {
         const uint32_t d = KO::digit(key[i], shift);
-        const uint32_t pos = s_local[d] + s_whist[warp * RADIX + d] + rank[i];
+        const uint32_t pos = cnt_w[d] + rank[i];
         rank[i] = pos;  // keep the tile position for the payload
         sk[pos] = key[i];
       }
     }
-    __syncthreads();  // (C) reordered keys and global bases ready
+    unit_sync<CL>();  // (C2) rank 0's unit prefixes visible; reordered keys ready
+    if (tid < RADIX) {
+      const int dg = tid;
+      const uint32_t excl = CL > 1 ? *cluster_peer(&s_excl[dg], 0u) : s_excl[dg];
+      s_gbase[dg] = s_binstart[dg] + excl + s_cpre[dg] - s_local[dg];
+    }
+    __syncthreads();  // (D) global bases ready
 
     // ---- write coalesced per-digit runs ----------------------------------------------
     // Every destination is checked against n: after a timed-out look-back the offsets are
@@ -463,13 +631,13 @@ __global__ void __launch_bounds__(NT, MINB) onesweep_pass_kernel(SortArgs args) 
         else if (idx < tile_n) v = vin[tile_base + idx];
         val[i] = v;
       }
-      __syncthreads();  // (D) all payloads read before they are overwritten
+      __syncthreads();  // (E1) all payloads read before they are overwritten
 #pragma unroll
       for (int i = 0; i < KPT; i++) {
         const int idx = wbase + i * 32 + lane;
         if (idx < tile_n) sv[rank[i]] = val[i];
       }
-      __syncthreads();  // (E)
+      __syncthreads();  // (E2)
 #pragma unroll
       for (int i = 0; i < KPT; i++) {
         const int s = i * NT + tid;
@@ -480,18 +648,58 @@ __global__ void __launch_bounds__(NT, MINB) onesweep_pass_kernel(SortArgs args) 
       }
     }
     if (out_of_range) atomicOr(err, uint32_t(DERR_BOUNDS));
+    if (trace) trace[6] = global_timer_ns();
     // The stage buffer was written through the generic proxy; a later bulk copy (async
     // proxy) refills it, so order the writes before the barrier.
     fence_proxy_async_smem();
-    __syncthreads();  // (F) shared memory free for the next tile
-    if (STAGES > 1) stage ^= 1;
-    else if (tid == 0) {
-      int tn = int(atomicAdd(tile_counter, 1u));
-      s_tile[0] = tn;
-      if (tn < num_tiles) onesweep_issue_tile<U, PAIRS, TILE>(smem, L::STAGE_BYTES, L::KEYS_BYTES, s_mbar, kin, vin, n, tn, 0);
-    }
-    if (STAGES == 1) __syncthreads();
+    __syncthreads();  // (F) shared memory free for the next sub-tile
+    stage ^= 1;
   }
+  // no CTA may exit while a peer can still read its shared memory
+  if (CL > 1) unit_sync<CL>();
+}
+
+// Verifies, on this GPU, that the ordered-atomic ranking gives lane-ordered (stable) ranks:
+// every warp ranks KPT x 32 digits with exactly the onesweep's code and compares each rank
+// with a brute-force count of earlier equal digits.  Patterns: uniform bytes, 4 values,
+// one value, and partial last rows.  Mismatches are added to *bad.
+template <int NT, int KPT>
+__global__ void __launch_bounds__(NT) rank_probe_kernel(uint32_t* bad, uint32_t seed) {
+  constexpr int NW = NT / 32;
+  __shared__ uint32_t cnt[NW][RADIX];
+  __shared__ uint16_t dig[NW][32 * KPT];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t mism = 0;
+  for (int pattern = 0; pattern < 4; pattern++) {
+    for (int i = lane; i < RADIX; i += 32) cnt[warp][i] = 0u;
+    const int valid_n = pattern == 3 ? (32 * KPT - 37) : 32 * KPT;
+    __syncwarp();
+    uint32_t x = seed ^ (blockIdx.x * 0x9E3779B9u) ^ (threadIdx.x * 0x85EBCA6Bu) ^ (pattern * 0xC2B2AE35u);
+    uint32_t d[KPT], r[KPT];
+#pragma unroll
+    for (int i = 0; i < KPT; i++) {
+      x ^= x << 13;
+      x ^= x >> 17;
+      x ^= x << 5;
+      d[i] = pattern == 0 ? (x & 255u) : pattern == 1 ? (x & 3u) : pattern == 2 ? 9u : ((x >> 3) & 7u);
+      dig[warp][i * 32 + lane] = uint16_t(d[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < KPT; i++) {
+      const bool valid = i * 32 + lane < valid_n;
+      r[i] = rank_in_warp<RANK_ORDERED_ATOMIC>(cnt[warp], nullptr, d[i], valid, i & 1, lane);
+    }
+    __syncwarp();
+    for (int i = 0; i < KPT; i++) {
+      const int pos = i * 32 + lane;
+      if (pos >= valid_n) continue;
+      uint32_t want = 0;
+      for (int q = 0; q < pos; q++) want += (dig[warp][q] == d[i]) ? 1u : 0u;
+      if (want != r[i]) mism++;
+    }
+    __syncwarp();
+  }
+  if (mism) atomicAdd(bad, mism);
 }
 
 // Copy B -> A when the result ended in the scratch buffer, and fold this sort's device

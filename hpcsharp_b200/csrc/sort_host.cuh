@@ -36,11 +36,16 @@ struct DevBuf {
 struct hpcs_ctx {
   int device = 0;
   int sms = 0;
+  int rank_mode = 1;  // hpcs::RankMode actually used
   hpcs_config cfg{};
   cudaStream_t stream = nullptr;
   cudaStream_t last_stream = nullptr;
   cudaEvent_t order_event = nullptr;
   size_t held_bytes = 0;
+  // tile trace (debug)
+  uint64_t* trace = nullptr;
+  int trace_pass = -1;
+  int trace_capacity = 0;
   // per-kernel timing
   bool profile = false;
   struct Timed {
@@ -71,27 +76,51 @@ struct KernelTimer {
 int enter_stream(hpcs_ctx* ctx, cudaStream_t s);
 uint32_t* device_error_word(hpcs_ctx* ctx);
 
-template <class U, class V>
+template <class U, class V, int MODE>
 struct SortConfig;
-// 32-bit keys: 512 threads x 16 keys = 8192-key tiles, 2 stages, 2 CTAs/SM.
+// Tile shapes (threads x keys per thread), prefetch stages, CTAs per SM and CTAs per
+// look-back unit (cluster size), per key/payload type and ranking mode.  The 32-bit
+// keys-only shape of the ordered-atomic ranking can be overridden at build time for
+// tuning sweeps.
+#ifndef HPCS_K32_NT
+#define HPCS_K32_NT 1024
+#endif
+#ifndef HPCS_K32_KPT
+#define HPCS_K32_KPT 16
+#endif
+#ifndef HPCS_K32_MINB
+#define HPCS_K32_MINB 1
+#endif
+#ifndef HPCS_CL
+#define HPCS_CL 1
+#endif
 template <>
-struct SortConfig<uint32_t, NoValue> {
-  static constexpr int NT = 512, KPT = 16, STAGES = 2, MINB = 2;
+struct SortConfig<uint32_t, NoValue, RANK_ORDERED_ATOMIC> {
+  static constexpr int NT = HPCS_K32_NT, KPT = HPCS_K32_KPT, STAGES = 2, MINB = HPCS_K32_MINB, CL = HPCS_CL;
 };
 template <>
-struct SortConfig<uint64_t, NoValue> {
-  static constexpr int NT = 512, KPT = 8, STAGES = 2, MINB = 2;
+struct SortConfig<uint32_t, NoValue, RANK_PEER_MASK> {  // + 32 KiB of lane masks
+  static constexpr int NT = 512, KPT = 16, STAGES = 2, MINB = 1, CL = 1;
 };
-template <>
-struct SortConfig<uint32_t, uint32_t> {
-  static constexpr int NT = 512, KPT = 8, STAGES = 2, MINB = 2;
+template <int MODE>
+struct SortConfig<uint64_t, NoValue, MODE> {
+  static constexpr int NT = 512, KPT = 8, STAGES = 2, MINB = 2, CL = HPCS_CL;
 };
-template <>
-struct SortConfig<uint64_t, uint32_t> {
-  static constexpr int NT = 512, KPT = 6, STAGES = 2, MINB = 2;
+template <int MODE>
+struct SortConfig<uint32_t, uint32_t, MODE> {
+  static constexpr int NT = 512, KPT = 8, STAGES = 2, MINB = 2, CL = HPCS_CL;
+};
+template <int MODE>
+struct SortConfig<uint64_t, uint32_t, MODE> {
+  static constexpr int NT = 512, KPT = 6, STAGES = 2, MINB = 2, CL = HPCS_CL;
 };
 
-constexpr int HIST_NT = 512;
+constexpr int HIST_NT = 1024;
+
+// Launches K1 (one CTA per SM, 128 KiB of lane-private counters).
+template <class U, int KIND>
+int launch_histogram(hpcs_ctx* ctx, const U* keys, int64_t n, uint32_t* hist_out, const SortArgs& args,
+                     int make_plan, cudaStream_t s);
 
 template <class Kernel>
 int occupancy_blocks(Kernel k, int nt, size_t smem) {
@@ -100,17 +129,75 @@ int occupancy_blocks(Kernel k, int nt, size_t smem) {
   return blocks > 0 ? blocks : 1;
 }
 
+template <class U, int KIND>
+int launch_histogram(hpcs_ctx* ctx, const U* keys, int64_t n, uint32_t* hist_out, const SortArgs& args,
+                     int make_plan, cudaStream_t s) {
+  auto k = hist_all_digits_kernel<U, KIND, HIST_NT>;
+  static int attr_set[64] = {0};
+  if (!attr_set[ctx->device & 63]) {
+    HPCS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(HistSmem<U>::BYTES)));
+    attr_set[ctx->device & 63] = 1;
+  }
+  const int64_t vec = n * int64_t(sizeof(U)) / 16;
+  const int64_t want = (vec + HIST_NT * 4 - 1) / (HIST_NT * 4);
+  const int grid = int(want < 1 ? 1 : (want > ctx->sms ? ctx->sms : want));
+  k<<<grid, HIST_NT, HistSmem<U>::BYTES, s>>>(keys, n, hist_out, args, make_plan);
+  HPCS_CUDA(cudaGetLastError());
+  return HPCS_OK;
+}
+
+// Onesweep launches for every digit pass, with the context's ranking mode.  Persistent
+// grid of as many CL-CTA clusters as fit on the GPU at once.
+template <class U, int KIND, class V, int MODE>
+int launch_onesweep_passes(hpcs_ctx* ctx, SortArgs args, cudaStream_t s) {
+  using C = SortConfig<U, V, MODE>;
+  using L = OnesweepSmem<U, V, C::NT, C::KPT, C::STAGES, MODE>;
+  constexpr int P = int(sizeof(U));
+  auto k = onesweep_pass_kernel<U, KIND, V, C::NT, C::KPT, C::STAGES, C::MINB, MODE, C::CL>;
+  static int clusters_by_dev[64] = {0};
+  int& clusters = clusters_by_dev[ctx->device & 63];
+  cudaLaunchConfig_t cfg{};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C::CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(C::NT, 1, 1);
+  cfg.dynamicSmemBytes = L::BYTES;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (!clusters) {
+    HPCS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::BYTES)));
+    if (C::CL > 1) HPCS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 0));
+    cfg.gridDim = dim3(C::CL * ctx->sms, 1, 1);
+    int mc = 0;
+    HPCS_CUDA(cudaOccupancyMaxActiveClusters(&mc, k, &cfg));
+    clusters = mc > 0 ? mc : 1;
+  }
+  const int64_t units = args.num_tiles;
+  const int grid_clusters = int(units < clusters ? units : clusters);
+  cfg.gridDim = dim3(grid_clusters * C::CL, 1, 1);
+  for (int p = 0; p < P; p++) {
+    args.pass = p;
+    KernelTimer kt(ctx, s, HPCS_K_ONESWEEP);
+    HPCS_CUDA(cudaLaunchKernelEx(&cfg, k, args));
+  }
+  return HPCS_OK;
+}
+
 // Enqueue a full LSD sort of n keys (and optional 4-byte items) in device memory.
 // keys/vals are sorted in place (with scratch B owned by the context).
 template <class U, int KIND, class V>
 int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t s) {
-  using C = SortConfig<U, V>;
-  using L = OnesweepSmem<U, V, C::NT, C::KPT, C::STAGES>;
+  using CA = SortConfig<U, V, RANK_ORDERED_ATOMIC>;
+  using CP = SortConfig<U, V, RANK_PEER_MASK>;
   constexpr bool PAIRS = !std::is_same<V, NoValue>::value;
-  constexpr int P = int(sizeof(U));
   if (n <= 1) return HPCS_OK;
   if (n > MAX_KEYS_PER_SORT) return fail(HPCS_ERR_RANGE, "n exceeds HPCS_MAX_KEYS");
-  const int64_t num_tiles = (n + L::TILE - 1) / L::TILE;
+  const int64_t unit = ctx->rank_mode == RANK_ORDERED_ATOMIC ? int64_t(CA::NT) * CA::KPT * CA::CL
+                                                             : int64_t(CP::NT) * CP::KPT * CP::CL;
+  const int64_t num_tiles = (n + unit - 1) / unit;  // look-back units
 
   // 16-byte alignment is required by the bulk copies; unaligned callers go through A'.
   U* a = keys;
@@ -148,39 +235,21 @@ int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t
   args.skip_trivial = ctx->cfg.skip_trivial_passes;
   args.poison_tile = ctx->cfg.poison_tile;
   args.spin_limit_ns = uint64_t(ctx->cfg.spin_limit_ns);
+  args.trace = ctx->trace;
+  args.trace_pass = ctx->trace_pass;
+  args.trace_capacity = ctx->trace_capacity;
 
   HPCS_CUDA(cudaMemsetAsync(args.plan, 0, sizeof(SortPlan), s));
 
   // K1: fused histogram + plan
   {
-    auto k = hist_all_digits_kernel<U, KIND, HIST_NT>;
-    static int hist_blocks = 0;
-    if (!hist_blocks) hist_blocks = occupancy_blocks(k, HIST_NT, 0);
-    const int64_t vec = n * int64_t(sizeof(U)) / 16;
-    int64_t want = (vec + HIST_NT * 4 - 1) / (HIST_NT * 4);
-    int64_t cap = int64_t(ctx->sms) * hist_blocks;
-    int grid = int(want < 1 ? 1 : (want > cap ? cap : want));
     KernelTimer kt(ctx, s, HPCS_K_HISTOGRAM);
-    k<<<grid, HIST_NT, 0, s>>>(a, n, &args.plan->hist[0][0], args, 1);
-    HPCS_CUDA(cudaGetLastError());
+    if ((rc = launch_histogram<U, KIND>(ctx, a, n, &args.plan->hist[0][0], args, 1, s)) != HPCS_OK) return rc;
   }
   // K3: one onesweep launch per digit
-  {
-    auto k = onesweep_pass_kernel<U, KIND, V, C::NT, C::KPT, C::STAGES, C::MINB>;
-    static int os_blocks = 0;
-    if (!os_blocks) {
-      HPCS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::BYTES)));
-      os_blocks = occupancy_blocks(k, C::NT, L::BYTES);
-    }
-    int64_t cap = int64_t(ctx->sms) * os_blocks;
-    int grid = int(num_tiles < cap ? num_tiles : cap);
-    for (int p = 0; p < P; p++) {
-      args.pass = p;
-      KernelTimer kt(ctx, s, HPCS_K_ONESWEEP);
-      k<<<grid, C::NT, L::BYTES, s>>>(args);
-      HPCS_CUDA(cudaGetLastError());
-    }
-  }
+  rc = ctx->rank_mode == RANK_ORDERED_ATOMIC ? launch_onesweep_passes<U, KIND, V, RANK_ORDERED_ATOMIC>(ctx, args, s)
+                                             : launch_onesweep_passes<U, KIND, V, RANK_PEER_MASK>(ctx, args, s);
+  if (rc != HPCS_OK) return rc;
   // finalize: result back into the caller's buffer if it ended in B; collect errors
   {
     int64_t want = (n + 255) / 256;

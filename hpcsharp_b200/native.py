@@ -13,7 +13,8 @@ import threading
 import numpy as np
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "libhpcs_gpu.so")
+# HPCS_GPU_LIB selects another build of the same library (e.g. a tuning variant).
+LIB_PATH = os.environ.get("HPCS_GPU_LIB") or os.path.join(_PKG, "libhpcs_gpu.so")
 
 HPCS_OK = 0
 HPCS_ERR_NULL = 1
@@ -61,7 +62,7 @@ class HpcsConfig(C.Structure):
     _fields_ = [
         ("pool_bytes", C.c_int64),
         ("skip_trivial_passes", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("rank_mode", C.c_int32),
         ("spin_limit_ns", C.c_int64),
         ("poison_tile", C.c_int32),
         ("reserved", C.c_int32 * 7),
@@ -94,6 +95,7 @@ def _declare(lib) -> None:
     lib.hpcs_ctx_synchronize.argtypes = [P]
     lib.hpcs_ctx_stream.argtypes = [P]
     lib.hpcs_ctx_stream.restype = P
+    lib.hpcs_ctx_rank_mode.argtypes = [P]
     lib.hpcs_last_error_message.restype = C.c_char_p
     lib.hpcs_status_string.argtypes = [I32]
     lib.hpcs_status_string.restype = C.c_char_p
@@ -106,6 +108,7 @@ def _declare(lib) -> None:
     lib.hpcs_histogram_byte_components_dev.argtypes = [P, I32, P, I64, P, P]
     lib.hpcs_ctx_profile_enable.argtypes = [P, I32]
     lib.hpcs_ctx_profile_read.argtypes = [P, C.POINTER(HpcsProfile)]
+    lib.hpcs_ctx_trace_tiles.argtypes = [P, P, I32, I32]
 
 
 def load():
@@ -159,13 +162,14 @@ class Context:
     """One hpcs_ctx: a CUDA stream plus grow-only scratch on one device."""
 
     def __init__(self, device: int = 0, *, pool_bytes: int = 0, skip_trivial_passes: bool = True,
-                 spin_limit_ns: int = 2_000_000_000, poison_tile: int = -1):
+                 spin_limit_ns: int = 2_000_000_000, poison_tile: int = -1, rank_mode: int = 0):
         self.lib = load()
         cfg = default_config()
         cfg.pool_bytes = pool_bytes
         cfg.skip_trivial_passes = 1 if skip_trivial_passes else 0
         cfg.spin_limit_ns = spin_limit_ns
         cfg.poison_tile = poison_tile
+        cfg.rank_mode = rank_mode
         h = C.c_void_p()
         check(self.lib.hpcs_ctx_create(device, C.byref(cfg), C.byref(h)))
         self.handle = h
@@ -189,6 +193,11 @@ class Context:
         self.close()
 
     @property
+    def rank_mode(self) -> int:
+        """0: ordered shared atomics (lane order verified on this GPU); 1: peer-mask ranking."""
+        return int(self.lib.hpcs_ctx_rank_mode(self.handle))
+
+    @property
     def stream(self) -> int:
         return self.lib.hpcs_ctx_stream(self.handle) or 0
 
@@ -204,6 +213,11 @@ class Context:
         p = HpcsProfile()
         check(self.lib.hpcs_ctx_profile_read(self.handle, C.byref(p)))
         return {k: (int(p.launches[v]), float(p.total_ms[v])) for k, v in KCLASS.items()}
+
+    def trace_tiles(self, buf, capacity_tiles: int, digit_pass: int) -> None:
+        """Attach a device buffer (int64, 7 words per tile) for the onesweep tile trace."""
+        check(self.lib.hpcs_ctx_trace_tiles(self.handle, _ptr(buf) if buf is not None else None,
+                                            capacity_tiles, digit_pass))
 
     # ---- host arrays (synchronous, in place) ----
     def sort(self, a: np.ndarray) -> np.ndarray:

@@ -65,7 +65,9 @@ typedef struct hpcs_ctx hpcs_ctx;
 typedef struct hpcs_config {
   int64_t pool_bytes;          /* device scratch budget of the context; 0 = unlimited */
   int32_t skip_trivial_passes; /* 1: skip a digit pass whose keys all share that digit */
-  int32_t reserved0;
+  int32_t rank_mode;           /* 0: one shared atomic per key, after this GPU passed the
+                                  lane-order probe at context creation (else as 1);
+                                  1: always the fully defined peer-mask ranking */
   int64_t spin_limit_ns;       /* bound on every device-side wait (default 2e9) */
   int32_t poison_tile;         /* test hook: tile that never publishes (-1 = off) */
   int32_t reserved[7];
@@ -79,6 +81,8 @@ int hpcs_ctx_destroy(hpcs_ctx* ctx);
 int hpcs_ctx_synchronize(hpcs_ctx* ctx);
 /* The context's own stream (a cudaStream_t). */
 void* hpcs_ctx_stream(hpcs_ctx* ctx);
+/* Ranking used by this context: 0 = ordered shared atomics (probe passed), 1 = peer mask. */
+int hpcs_ctx_rank_mode(hpcs_ctx* ctx);
 const char* hpcs_last_error_message(void);
 const char* hpcs_status_string(int status);
 int hpcs_abi_version(void);
@@ -103,6 +107,11 @@ typedef struct hpcs_profile {
 } hpcs_profile;
 
 int hpcs_ctx_profile_enable(hpcs_ctx* ctx, int enable);
+/* Tile trace (debug): while set, each onesweep launch of digit pass `pass` writes 7 words
+ * per tile t < capacity_tiles at trace[7*t]: tile id, SM id, and %globaltimer (ns) at
+ * start, data ready, ranked, look-back done (digit 0), end of scatter.  trace is device
+ * memory; NULL turns tracing off. */
+int hpcs_ctx_trace_tiles(hpcs_ctx* ctx, uint64_t* trace, int capacity_tiles, int pass);
 int hpcs_ctx_profile_read(hpcs_ctx* ctx, hpcs_profile* out);
 
 /* ---- plain sort, host arrays, in place ----------------------------------------------

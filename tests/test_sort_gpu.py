@@ -190,21 +190,48 @@ def test_pool_budget_is_enforced(orc):
 
 
 def test_lookback_wait_is_bounded(orc):
-    """A tile that never publishes (host-set test hook) makes every later tile's
+    """A look-back unit that never publishes (host-set test hook) makes every later unit's
     look-back run out after the spin limit: the call returns HPCS_ERR_DEVICE_TIMEOUT and
     the context stays usable."""
+    n = 600_000  # several look-back units after the poisoned one, whatever the unit size
     c = native.Context(0, spin_limit_ns=20_000_000, poison_tile=1)
     try:
-        a = datagen.u32_uniform(8192 * 6, seed=1)
+        a = datagen.u32_uniform(n, seed=1)
         with pytest.raises(native.DeviceTimeoutError):
             c.sort(a)
     finally:
         c.close()
     c2 = native.Context(0)
     try:
-        a = datagen.u32_uniform(8192 * 6, seed=1)
+        a = datagen.u32_uniform(n, seed=1)
         want = oracle_sorted(orc, a)
         c2.sort(a)
         assert_same_bits(a, want)
     finally:
         c2.close()
+
+
+def test_rank_probe_selects_a_mode(ctx):
+    # 0 = ordered shared atomics (lane order verified on this GPU), 1 = peer-mask ranking
+    assert ctx.rank_mode in (0, 1)
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+def test_peer_mask_ranking_parity(orc, dt):
+    """The fully defined peer-mask ranking gives the same bits as the oracle."""
+    c = native.Context(0, rank_mode=1)
+    try:
+        assert c.rank_mode == 1
+        for n in (4097, 300_001):
+            a = datagen.by_name(dt, n, seed=55 + n)
+            want = oracle_sorted(orc, a)
+            got = a.copy()
+            c.sort(got)
+            assert_same_bits(got, want)
+        keys = _adversarial(dt if dt in ("u32", "i32", "f32", "u64") else "u64", 100_003, "dups_mod_1000")
+        want = oracle_sorted(orc, keys)
+        got = keys.copy()
+        c.sort(got)
+        assert_same_bits(got, want)
+    finally:
+        c.close()
