@@ -25,7 +25,7 @@ NVCC_FLAGS = [
     "--expt-relaxed-constexpr",
 ]
 
-GPU_SOURCES = ["capi.cu"]
+GPU_SOURCES = ["capi.cu", "noalloc.cu"]
 GPU_DEPS = ["common.cuh", "radix_kernels.cuh", "sort_host.cuh"]
 
 

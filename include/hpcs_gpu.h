@@ -179,6 +179,27 @@ int hpcs_histogram_byte_components_f64(hpcs_ctx* ctx, const double* a, int64_t l
 int hpcs_histogram_byte_components_dev(hpcs_ctx* ctx, int dtype, const void* a, int64_t n, uint32_t* counts,
                                        void* stream);
 
+/* ---- uint32 device sort that allocates nothing --------------------------------------
+ * No counterpart in the reference (HPCsharp allocates managed arrays per call).  For callers
+ * that cannot allocate GPU memory: code whose framework owns every device allocation (a
+ * fixed arena or a capped caching allocator), or code on a path where cudaMalloc/cudaFree and
+ * their implicit device synchronisation are not allowed.  Sorts n <= HPCS_NOALLOC_MAX_KEYS
+ * uint32 keys at `keys` (device memory, 16-byte aligned) in place, stable and ascending, with
+ * all scratch taken from a fixed array compiled into the library; every GPU that loads the
+ * library holds that array (about 4.3 MB) until the process exits.  No context is needed and
+ * no cudaMalloc, cudaFree or other allocating routine is called.
+ *   - Larger n returns HPCS_ERR_RANGE; an unaligned pointer HPCS_ERR_UNSUPPORTED.
+ *   - Runs on `stream` (a cudaStream_t of the current device) and returns when the sort has
+ *     finished, reporting a device-side wait that ran out as HPCS_ERR_DEVICE_TIMEOUT.
+ *   - The first call on a device also does a one-time set-up on the current device (it
+ *     looks up the scratch array's device address and sets kernel attributes); make that
+ *     first call before any stream capture.
+ *   - All calls on a device share the one scratch array, which keeps the last call's
+ *     contents (each call clears what must start at zero).  Calls that overlap on the GPU --
+ *     from several streams or host threads at once -- race and corrupt each other. */
+#define HPCS_NOALLOC_MAX_KEYS ((int64_t)1048576) /* 2^20 keys */
+int hpcs_sort_u32_dev_noalloc(uint32_t* keys, int64_t n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,63 @@
+"""The uint32 device sort that allocates nothing (hpcs_sort_u32_dev_noalloc), called through
+the C ABI, must give the same bits as the regular context-based entry point
+(hpcs_sort_u32_dev): integer keys, so the tolerance is exact equality.  It is meant for callers
+that cannot allocate GPU memory -- their framework owns every device allocation, or
+cudaMalloc/cudaFree are not allowed where they call -- and takes all its scratch from a fixed
+array compiled into the library, so it is limited to HPCS_NOALLOC_MAX_KEYS keys.
+
+This file is collected last so that a failure here cannot hide the other tests."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from hpcsharp_b200 import datagen, native
+from tests.gpu_util import from_dev, to_dev
+
+pytestmark = pytest.mark.gpu
+
+NOALLOC_MAX_KEYS = 1 << 20
+
+
+def _entry():
+    lib = native.load()
+    fn = lib.hpcs_sort_u32_dev_noalloc
+    fn.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+    fn.restype = C.c_int
+    return lib, fn
+
+
+def test_no_alloc_sort_matches_context_sort_twice():
+    import torch
+
+    lib, fn = _entry()
+    ctx = native.Context(0)
+    try:
+        stream = torch.cuda.current_stream().cuda_stream
+        # two calls in a row, the second smaller (the scratch keeps the first call's contents)
+        for n, seed in ((NOALLOC_MAX_KEYS, 101), (777_777, 202)):
+            a = datagen.u32_uniform(n, seed=seed)
+            t_noalloc = to_dev(a)
+            t_regular = to_dev(a)
+            rc = fn(t_noalloc.data_ptr(), n, stream)
+            assert rc == native.HPCS_OK, lib.hpcs_last_error_message()
+            ctx.sort_dev(t_regular, dtype="u32", stream=stream)
+            torch.cuda.synchronize()
+            ctx.synchronize()
+            got = from_dev(t_noalloc, np.uint32)
+            want = from_dev(t_regular, np.uint32)
+            np.testing.assert_array_equal(got, want)
+            assert np.all(got[1:] >= got[:-1])
+    finally:
+        ctx.close()
+
+
+def test_no_alloc_sort_rejects_too_many_keys():
+    import torch
+
+    lib, fn = _entry()
+    t = torch.zeros(NOALLOC_MAX_KEYS + 1, dtype=torch.int32, device="cuda")
+    rc = fn(t.data_ptr(), NOALLOC_MAX_KEYS + 1, torch.cuda.current_stream().cuda_stream)
+    assert rc == native.HPCS_ERR_RANGE
+    assert b"HPCS_NOALLOC_MAX_KEYS" in lib.hpcs_last_error_message()
+    assert fn(None, 10, None) == native.HPCS_ERR_NULL
