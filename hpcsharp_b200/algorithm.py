@@ -90,3 +90,23 @@ def HistogramByteComponentsPar(inArray: np.ndarray, l: int, r: int, parallelThre
 def HistogramByteComponents(inArray: np.ndarray, l: int, r: int):
     """int[P][256] digit counts of inArray[l..r] (inclusive)."""
     return HistogramByteComponentsPar(inArray, l, r).astype(np.int32)
+
+
+def SelectTopK(arrayToBeSelected: np.ndarray, *args) -> None:
+    """SelectTopK(a, k) or SelectTopK(a, start, length, k) (SelectionTopKRadix.cs:142-171),
+    in place: afterwards a[k] is the k-th smallest and a[k..] the largest of the (sub)array.
+    In the (start, length, k) form k indexes the whole array, as in the reference."""
+    _require(arrayToBeSelected, "arrayToBeSelected")
+    a = arrayToBeSelected
+    if len(args) == 1:
+        k = args[0]
+        if a.size <= 0 or k < 0 or k >= a.size:
+            raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "k must be between start and (start + length)")
+        default_context().select_topk(a, k)
+        return
+    start, length, k = args
+    if start < 0 or length <= 0 or start + length > a.size:
+        raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "l or r are invalid")
+    if k < start or k >= start + length:
+        raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "k must be between start and (start + length)")
+    default_context().select_topk(a[start:start + length], k - start)

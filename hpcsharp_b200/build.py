@@ -26,7 +26,7 @@ NVCC_FLAGS = [
 ]
 
 GPU_SOURCES = ["capi.cu", "noalloc.cu"]
-GPU_DEPS = ["common.cuh", "radix_kernels.cuh", "sort_host.cuh"]
+GPU_DEPS = ["common.cuh", "radix_kernels.cuh", "sort_host.cuh", "topk.cuh"]
 
 
 def _nvcc() -> str:

@@ -7,6 +7,7 @@
 
 #include "../../include/hpcs_gpu.h"
 #include "sort_host.cuh"
+#include "topk.cuh"
 
 namespace hpcs {
 
@@ -261,6 +262,149 @@ int histogram_host(hpcs_ctx* ctx, const T* a, int64_t l, int64_t r, uint32_t* co
   return HPCS_OK;
 }
 
+// Radix select of the key of 0-based rank `rank` among n keys at device pointer d.  Leaves
+// the SelectState in ctx->aux1 (prefix = the ordered bits of the selected key, less/eq counts).
+template <class U, int KIND>
+int enqueue_select(hpcs_ctx* ctx, const U* d, int64_t n, int64_t rank, cudaStream_t s, SelectState** out) {
+  constexpr int BITS = int(sizeof(U) * 8);
+  constexpr int LEVELS = BITS / 8;
+  int rc;
+  if ((rc = ensure(ctx, ctx->aux1, sizeof(SelectState))) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->aux0, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
+  SelectState* st = static_cast<SelectState*>(ctx->aux1.ptr);
+  U* cand = static_cast<U*>(ctx->aux0.ptr);
+  KernelTimer kt(ctx, s, HPCS_K_TOPK);
+  select_init_kernel<<<1, 256, 0, s>>>(st, rank);
+  const int64_t want = (n + SEL_NT * 4 - 1) / (SEL_NT * 4);
+  const int grid = int(want < 1 ? 1 : (want > int64_t(ctx->sms) * 2 ? int64_t(ctx->sms) * 2 : want));
+  select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, nullptr, n, st, BITS - 8);
+  select_pick_kernel<U><<<1, 256, 0, s>>>(st, BITS - 8, LEVELS == 1);
+  select_compact_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, cand, st);
+  for (int l = 1; l < LEVELS; l++) {
+    const int shift = BITS - 8 * (l + 1);
+    select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(cand, &st->cand_count, 0, st, shift);
+    select_pick_kernel<U><<<1, 256, 0, s>>>(st, shift, l == LEVELS - 1);
+  }
+  HPCS_CUDA(cudaGetLastError());
+  *out = st;
+  return HPCS_OK;
+}
+
+// Stable three-way partition of d[0..n) around the selected key into out.
+template <class U, int KIND>
+int enqueue_partition(hpcs_ctx* ctx, const U* d, int64_t n, SelectState* st, U* out, cudaStream_t s) {
+  const int64_t tiles = (n + PART_TILE - 1) / PART_TILE;
+  int rc;
+  if ((rc = ensure(ctx, ctx->aux2, size_t(tiles) * 3 * 4)) != HPCS_OK) return rc;
+  uint32_t* tc = static_cast<uint32_t*>(ctx->aux2.ptr);
+  KernelTimer kt(ctx, s, HPCS_K_TOPK);
+  partition_count_kernel<U, KIND><<<int(tiles), PART_NT, 0, s>>>(d, n, st, tc);
+  partition_scan_kernel<<<1, 1024, 0, s>>>(tc, tiles, st, n);
+  partition_scatter_kernel<U, KIND><<<int(tiles), PART_NT, 0, s>>>(d, n, st, tc, out);
+  HPCS_CUDA(cudaGetLastError());
+  return HPCS_OK;
+}
+
+int check_select_args(hpcs_ctx* ctx, const void* a, int64_t n, int64_t k) {
+  if (!ctx) return fail(HPCS_ERR_NULL, "ctx is NULL");
+  if (!a) return fail(HPCS_ERR_NULL, "array is NULL");
+  // SelectTopK(a, k): length must be positive and k a valid index (SelectionTopKRadix.cs:164-167;
+  // k == Length passes the reference's check but then indexes past its bins).
+  if (n <= 0) return fail(HPCS_ERR_RANGE, "array length is invalid");
+  if (n > HPCS_MAX_KEYS) return fail(HPCS_ERR_RANGE, "length exceeds HPCS_MAX_KEYS");
+  if (k < 0 || k >= n) return fail(HPCS_ERR_RANGE, "k must be in [0, length)");
+  return HPCS_OK;
+}
+
+template <class T, class U, int KIND>
+int select_topk_host(hpcs_ctx* ctx, T* a, int64_t n, int64_t k) {
+  int rc = check_select_args(ctx, a, n, k);
+  if (rc != HPCS_OK) return rc;
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = ctx->stream;
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->keys_a, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->keys_b, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
+  U* d = static_cast<U*>(ctx->keys_a.ptr);
+  U* o = static_cast<U*>(ctx->keys_b.ptr);
+  HPCS_CUDA(cudaMemcpyAsync(d, a, size_t(n) * sizeof(U), cudaMemcpyHostToDevice, s));
+  SelectState* st = nullptr;
+  if ((rc = enqueue_select<U, KIND>(ctx, d, n, k, s, &st)) != HPCS_OK) return rc;
+  if ((rc = enqueue_partition<U, KIND>(ctx, d, n, st, o, s)) != HPCS_OK) return rc;
+  HPCS_CUDA(cudaMemcpyAsync(a, o, size_t(n) * sizeof(U), cudaMemcpyDeviceToHost, s));
+  HPCS_CUDA(cudaStreamSynchronize(s));
+  return check_device_errors(ctx);
+}
+
+template <class T, class U, int KIND>
+int select_topk_dev(hpcs_ctx* ctx, T* a, int64_t n, int64_t k, void* stream) {
+  int rc = check_select_args(ctx, a, n, k);
+  if (rc != HPCS_OK) return rc;
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = pick_stream(ctx, stream);
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->keys_b, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
+  U* d = reinterpret_cast<U*>(a);
+  U* o = static_cast<U*>(ctx->keys_b.ptr);
+  SelectState* st = nullptr;
+  if ((rc = enqueue_select<U, KIND>(ctx, d, n, k, s, &st)) != HPCS_OK) return rc;
+  if ((rc = enqueue_partition<U, KIND>(ctx, d, n, st, o, s)) != HPCS_OK) return rc;
+  HPCS_CUDA(cudaMemcpyAsync(d, o, size_t(n) * sizeof(U), cudaMemcpyDeviceToDevice, s));
+  return HPCS_OK;
+}
+
+// The k largest of in[0..n) into out[0..k), ascending (device pointers).
+template <class T, class U, int KIND>
+int topk_largest_enqueue(hpcs_ctx* ctx, const U* d, int64_t n, int64_t k, U* out, cudaStream_t s) {
+  SelectState* st = nullptr;
+  int rc;
+  if ((rc = enqueue_select<U, KIND>(ctx, d, n, n - k, s, &st)) != HPCS_OK) return rc;
+  const int64_t want = (n + SEL_NT * 4 - 1) / (SEL_NT * 4);
+  const int grid = int(want < 1 ? 1 : (want > int64_t(ctx->sms) * 2 ? int64_t(ctx->sms) * 2 : want));
+  {
+    KernelTimer kt(ctx, s, HPCS_K_TOPK);
+    topk_gather_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, k, st, out);
+    HPCS_CUDA(cudaGetLastError());
+  }
+  return enqueue_sort<U, KIND, NoValue>(ctx, out, nullptr, k, s);
+}
+
+int check_topk_args(hpcs_ctx* ctx, const void* in, const void* out, int64_t n, int64_t k) {
+  if (!ctx) return fail(HPCS_ERR_NULL, "ctx is NULL");
+  if (!in || !out) return fail(HPCS_ERR_NULL, "array is NULL");
+  if (n < 0 || n > HPCS_MAX_KEYS) return fail(HPCS_ERR_RANGE, "length out of range");
+  if (k < 0 || k > n) return fail(HPCS_ERR_RANGE, "k must be in [0, length]");
+  return HPCS_OK;
+}
+
+template <class T, class U, int KIND>
+int topk_largest_dev(hpcs_ctx* ctx, const T* in, int64_t n, int64_t k, T* out, void* stream) {
+  int rc = check_topk_args(ctx, in, out, n, k);
+  if (rc != HPCS_OK || k == 0) return rc;
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = pick_stream(ctx, stream);
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  return topk_largest_enqueue<T, U, KIND>(ctx, reinterpret_cast<const U*>(in), n, k, reinterpret_cast<U*>(out), s);
+}
+
+template <class T, class U, int KIND>
+int topk_largest_host(hpcs_ctx* ctx, const T* in, int64_t n, int64_t k, T* out) {
+  int rc = check_topk_args(ctx, in, out, n, k);
+  if (rc != HPCS_OK || k == 0) return rc;
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = ctx->stream;
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->keys_a, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->vals_a, size_t(k) * sizeof(U))) != HPCS_OK) return rc;
+  U* d = static_cast<U*>(ctx->keys_a.ptr);
+  U* o = static_cast<U*>(ctx->vals_a.ptr);
+  HPCS_CUDA(cudaMemcpyAsync(d, in, size_t(n) * sizeof(U), cudaMemcpyHostToDevice, s));
+  if ((rc = topk_largest_enqueue<T, U, KIND>(ctx, d, n, k, o, s)) != HPCS_OK) return rc;
+  HPCS_CUDA(cudaMemcpyAsync(out, o, size_t(k) * sizeof(U), cudaMemcpyDeviceToHost, s));
+  HPCS_CUDA(cudaStreamSynchronize(s));
+  return check_device_errors(ctx);
+}
+
 }  // namespace
 }  // namespace hpcs
 
@@ -494,6 +638,26 @@ int hpcs_histogram_byte_components_i64(hpcs_ctx* c, const int64_t* a, int64_t l,
 int hpcs_histogram_byte_components_f64(hpcs_ctx* c, const double* a, int64_t l, int64_t r, uint32_t* o) {
   return histogram_host<double, uint64_t, KIND_FLOAT>(c, a, l, r, o);
 }
+
+#define HPCS_TOPK_EXPORTS(NAME, T, U, KIND)                                                          \
+  int hpcs_select_topk_##NAME(hpcs_ctx* c, T* a, int64_t n, int64_t k) {                            \
+    return select_topk_host<T, U, KIND>(c, a, n, k);                                                 \
+  }                                                                                                  \
+  int hpcs_select_topk_##NAME##_dev(hpcs_ctx* c, T* a, int64_t n, int64_t k, void* s) {             \
+    return select_topk_dev<T, U, KIND>(c, a, n, k, s);                                               \
+  }                                                                                                  \
+  int hpcs_topk_largest_##NAME(hpcs_ctx* c, const T* in, int64_t n, int64_t k, T* out) {            \
+    return topk_largest_host<T, U, KIND>(c, in, n, k, out);                                          \
+  }                                                                                                  \
+  int hpcs_topk_largest_##NAME##_dev(hpcs_ctx* c, const T* in, int64_t n, int64_t k, T* out, void* s) { \
+    return topk_largest_dev<T, U, KIND>(c, in, n, k, out, s);                                        \
+  }
+HPCS_TOPK_EXPORTS(u32, uint32_t, uint32_t, KIND_UNSIGNED)
+HPCS_TOPK_EXPORTS(i32, int32_t, uint32_t, KIND_SIGNED)
+HPCS_TOPK_EXPORTS(f32, float, uint32_t, KIND_FLOAT)
+HPCS_TOPK_EXPORTS(u64, uint64_t, uint64_t, KIND_UNSIGNED)
+HPCS_TOPK_EXPORTS(i64, int64_t, uint64_t, KIND_SIGNED)
+HPCS_TOPK_EXPORTS(f64, double, uint64_t, KIND_FLOAT)
 
 int hpcs_histogram_byte_components_dev(hpcs_ctx* ctx, int dtype, const void* a, int64_t n, uint32_t* counts,
                                        void* stream) {

@@ -105,6 +105,10 @@ def _declare(lib) -> None:
         getattr(lib, f"hpcs_sort_pairs_{t}").argtypes = [P, P, P, I64]
         getattr(lib, f"hpcs_sort_pairs_{t}_dev").argtypes = [P, P, P, I64, P]
         getattr(lib, f"hpcs_histogram_byte_components_{t}").argtypes = [P, P, I64, I64, P]
+        getattr(lib, f"hpcs_select_topk_{t}").argtypes = [P, P, I64, I64]
+        getattr(lib, f"hpcs_select_topk_{t}_dev").argtypes = [P, P, I64, I64, P]
+        getattr(lib, f"hpcs_topk_largest_{t}").argtypes = [P, P, I64, I64, P]
+        getattr(lib, f"hpcs_topk_largest_{t}_dev").argtypes = [P, P, I64, I64, P, P]
     lib.hpcs_histogram_byte_components_dev.argtypes = [P, I32, P, I64, P, P]
     lib.hpcs_ctx_profile_enable.argtypes = [P, I32]
     lib.hpcs_ctx_profile_read.argtypes = [P, C.POINTER(HpcsProfile)]
@@ -241,6 +245,20 @@ class Context:
         check(getattr(self.lib, f"hpcs_histogram_byte_components_{t}")(self.handle, _ptr(a), l, r, _ptr(counts)))
         return counts
 
+    def select_topk(self, a: np.ndarray, k: int) -> np.ndarray:
+        """SelectTopK(a, k) in place: a[k] = k-th smallest, a[k:] = the n-k largest."""
+        t = dtype_name(a.dtype)
+        check(getattr(self.lib, f"hpcs_select_topk_{t}")(self.handle, _ptr(a), a.size, k))
+        return a
+
+    def topk_largest(self, a: np.ndarray, k: int) -> np.ndarray:
+        """The k largest keys of a, ascending."""
+        t = dtype_name(a.dtype)
+        out = np.empty(k, dtype=a.dtype)
+        if k:
+            check(getattr(self.lib, f"hpcs_topk_largest_{t}")(self.handle, _ptr(a), a.size, k, _ptr(out)))
+        return out
+
     # ---- device tensors (asynchronous on `stream`, default: the context's stream) ----
     def sort_dev(self, t, dtype: str | None = None, stream: int | None = None) -> None:
         name = dtype or _torch_dtype_name(t)
@@ -250,6 +268,15 @@ class Context:
         name = dtype or _torch_dtype_name(keys)
         check(getattr(self.lib, f"hpcs_sort_pairs_{name}_dev")(self.handle, _ptr(keys), _ptr(items), keys.numel(),
                                                                 stream))
+
+    def select_topk_dev(self, t, k: int, dtype: str | None = None, stream: int | None = None) -> None:
+        name = dtype or _torch_dtype_name(t)
+        check(getattr(self.lib, f"hpcs_select_topk_{name}_dev")(self.handle, _ptr(t), t.numel(), k, stream))
+
+    def topk_largest_dev(self, t, k: int, out, dtype: str | None = None, stream: int | None = None) -> None:
+        name = dtype or _torch_dtype_name(t)
+        check(getattr(self.lib, f"hpcs_topk_largest_{name}_dev")(self.handle, _ptr(t), t.numel(), k, _ptr(out),
+                                                                 stream))
 
     def histogram_dev(self, t, counts, dtype: str | None = None, stream: int | None = None) -> None:
         name = dtype or _torch_dtype_name(t)

@@ -179,6 +179,41 @@ int hpcs_histogram_byte_components_f64(hpcs_ctx* ctx, const double* a, int64_t l
 int hpcs_histogram_byte_components_dev(hpcs_ctx* ctx, int dtype, const void* a, int64_t n, uint32_t* counts,
                                        void* stream);
 
+/* ---- radix top-k ---------------------------------------------------------------------
+ * Algorithm.SelectTopK(this uint[] a, int k) SelectionTopKRadix.cs:160-171 (and the
+ * (a, start, length, k) form :142-153 via a pointer offset): afterwards a[k] is the k-th
+ * smallest key (0-based) and a[k..n-1] holds exactly the multiset of the n-k largest.  Here
+ * a[0..k-1] also holds the k smallest (the reference clobbers that prefix).  n <= 0 or k
+ * outside [0, n) -> HPCS_ERR_RANGE (the reference accepts k == n but then reads past its
+ * bins).  The reference has uint only; the other dtypes use the sort's order transforms. */
+int hpcs_select_topk_u32(hpcs_ctx* ctx, uint32_t* a, int64_t n, int64_t k);
+int hpcs_select_topk_i32(hpcs_ctx* ctx, int32_t* a, int64_t n, int64_t k);
+int hpcs_select_topk_f32(hpcs_ctx* ctx, float* a, int64_t n, int64_t k);
+int hpcs_select_topk_u64(hpcs_ctx* ctx, uint64_t* a, int64_t n, int64_t k);
+int hpcs_select_topk_i64(hpcs_ctx* ctx, int64_t* a, int64_t n, int64_t k);
+int hpcs_select_topk_f64(hpcs_ctx* ctx, double* a, int64_t n, int64_t k);
+int hpcs_select_topk_u32_dev(hpcs_ctx* ctx, uint32_t* a, int64_t n, int64_t k, void* stream);
+int hpcs_select_topk_i32_dev(hpcs_ctx* ctx, int32_t* a, int64_t n, int64_t k, void* stream);
+int hpcs_select_topk_f32_dev(hpcs_ctx* ctx, float* a, int64_t n, int64_t k, void* stream);
+int hpcs_select_topk_u64_dev(hpcs_ctx* ctx, uint64_t* a, int64_t n, int64_t k, void* stream);
+int hpcs_select_topk_i64_dev(hpcs_ctx* ctx, int64_t* a, int64_t n, int64_t k, void* stream);
+int hpcs_select_topk_f64_dev(hpcs_ctx* ctx, double* a, int64_t n, int64_t k, void* stream);
+/* The k largest of in[0..n) written to out[0..k) in ascending order (the top-k of a serving
+ * request; equals the reference's a[n-k..n-1] after SelectTopK(a, n-k), sorted).  k in
+ * [0, n]. */
+int hpcs_topk_largest_u32(hpcs_ctx* ctx, const uint32_t* in, int64_t n, int64_t k, uint32_t* out);
+int hpcs_topk_largest_i32(hpcs_ctx* ctx, const int32_t* in, int64_t n, int64_t k, int32_t* out);
+int hpcs_topk_largest_f32(hpcs_ctx* ctx, const float* in, int64_t n, int64_t k, float* out);
+int hpcs_topk_largest_u64(hpcs_ctx* ctx, const uint64_t* in, int64_t n, int64_t k, uint64_t* out);
+int hpcs_topk_largest_i64(hpcs_ctx* ctx, const int64_t* in, int64_t n, int64_t k, int64_t* out);
+int hpcs_topk_largest_f64(hpcs_ctx* ctx, const double* in, int64_t n, int64_t k, double* out);
+int hpcs_topk_largest_u32_dev(hpcs_ctx* ctx, const uint32_t* in, int64_t n, int64_t k, uint32_t* out, void* stream);
+int hpcs_topk_largest_i32_dev(hpcs_ctx* ctx, const int32_t* in, int64_t n, int64_t k, int32_t* out, void* stream);
+int hpcs_topk_largest_f32_dev(hpcs_ctx* ctx, const float* in, int64_t n, int64_t k, float* out, void* stream);
+int hpcs_topk_largest_u64_dev(hpcs_ctx* ctx, const uint64_t* in, int64_t n, int64_t k, uint64_t* out, void* stream);
+int hpcs_topk_largest_i64_dev(hpcs_ctx* ctx, const int64_t* in, int64_t n, int64_t k, int64_t* out, void* stream);
+int hpcs_topk_largest_f64_dev(hpcs_ctx* ctx, const double* in, int64_t n, int64_t k, double* out, void* stream);
+
 /* ---- uint32 device sort that allocates nothing --------------------------------------
  * No counterpart in the reference (HPCsharp allocates managed arrays per call).  For callers
  * that cannot allocate GPU memory: code whose framework owns every device allocation (a
