@@ -25,8 +25,9 @@ NVCC_FLAGS = [
     "--expt-relaxed-constexpr",
 ]
 
-GPU_SOURCES = ["capi.cu", "noalloc.cu"]
-GPU_DEPS = ["common.cuh", "radix_kernels.cuh", "sort_host.cuh", "topk.cuh"]
+GPU_SOURCES = ["capi.cu", "noalloc.cu", "segmented_host.cu", "serve.cu"]
+GPU_DEPS = ["common.cuh", "radix_kernels.cuh", "sort_host.cuh", "topk.cuh", "segmented.cuh", "topk_host.cuh",
+            "segmented_host.cuh"]
 
 
 def _nvcc() -> str:

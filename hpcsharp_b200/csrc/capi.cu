@@ -7,7 +7,7 @@
 
 #include "../../include/hpcs_gpu.h"
 #include "sort_host.cuh"
-#include "topk.cuh"
+#include "topk_host.cuh"
 
 namespace hpcs {
 
@@ -30,6 +30,7 @@ int cuda_fail(cudaError_t e, const char* what) {
 
 int ensure(hpcs_ctx* ctx, DevBuf& b, size_t bytes) {
   if (b.bytes >= bytes) return HPCS_OK;
+  if (b.borrowed) return fail(HPCS_ERR_OOM, "borrowed scratch is smaller than the request needs");
   size_t want = bytes < 256 ? 256 : bytes;
   if (ctx->cfg.pool_bytes > 0 && ctx->held_bytes - b.bytes + want > size_t(ctx->cfg.pool_bytes))
     return fail(HPCS_ERR_OOM, "request exceeds the context's pool_bytes budget");
@@ -262,49 +263,6 @@ int histogram_host(hpcs_ctx* ctx, const T* a, int64_t l, int64_t r, uint32_t* co
   return HPCS_OK;
 }
 
-// Radix select of the key of 0-based rank `rank` among n keys at device pointer d.  Leaves
-// the SelectState in ctx->aux1 (prefix = the ordered bits of the selected key, less/eq counts).
-template <class U, int KIND>
-int enqueue_select(hpcs_ctx* ctx, const U* d, int64_t n, int64_t rank, cudaStream_t s, SelectState** out) {
-  constexpr int BITS = int(sizeof(U) * 8);
-  constexpr int LEVELS = BITS / 8;
-  int rc;
-  if ((rc = ensure(ctx, ctx->aux1, sizeof(SelectState))) != HPCS_OK) return rc;
-  if ((rc = ensure(ctx, ctx->aux0, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
-  SelectState* st = static_cast<SelectState*>(ctx->aux1.ptr);
-  U* cand = static_cast<U*>(ctx->aux0.ptr);
-  KernelTimer kt(ctx, s, HPCS_K_TOPK);
-  select_init_kernel<<<1, 256, 0, s>>>(st, rank);
-  const int64_t want = (n + SEL_NT * 4 - 1) / (SEL_NT * 4);
-  const int grid = int(want < 1 ? 1 : (want > int64_t(ctx->sms) * 2 ? int64_t(ctx->sms) * 2 : want));
-  select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, nullptr, n, st, BITS - 8);
-  select_pick_kernel<U><<<1, 256, 0, s>>>(st, BITS - 8, LEVELS == 1);
-  select_compact_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, cand, st);
-  for (int l = 1; l < LEVELS; l++) {
-    const int shift = BITS - 8 * (l + 1);
-    select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(cand, &st->cand_count, 0, st, shift);
-    select_pick_kernel<U><<<1, 256, 0, s>>>(st, shift, l == LEVELS - 1);
-  }
-  HPCS_CUDA(cudaGetLastError());
-  *out = st;
-  return HPCS_OK;
-}
-
-// Stable three-way partition of d[0..n) around the selected key into out.
-template <class U, int KIND>
-int enqueue_partition(hpcs_ctx* ctx, const U* d, int64_t n, SelectState* st, U* out, cudaStream_t s) {
-  const int64_t tiles = (n + PART_TILE - 1) / PART_TILE;
-  int rc;
-  if ((rc = ensure(ctx, ctx->aux2, size_t(tiles) * 3 * 4)) != HPCS_OK) return rc;
-  uint32_t* tc = static_cast<uint32_t*>(ctx->aux2.ptr);
-  KernelTimer kt(ctx, s, HPCS_K_TOPK);
-  partition_count_kernel<U, KIND><<<int(tiles), PART_NT, 0, s>>>(d, n, st, tc);
-  partition_scan_kernel<<<1, 1024, 0, s>>>(tc, tiles, st, n);
-  partition_scatter_kernel<U, KIND><<<int(tiles), PART_NT, 0, s>>>(d, n, st, tc, out);
-  HPCS_CUDA(cudaGetLastError());
-  return HPCS_OK;
-}
-
 int check_select_args(hpcs_ctx* ctx, const void* a, int64_t n, int64_t k) {
   if (!ctx) return fail(HPCS_ERR_NULL, "ctx is NULL");
   if (!a) return fail(HPCS_ERR_NULL, "array is NULL");
@@ -351,22 +309,6 @@ int select_topk_dev(hpcs_ctx* ctx, T* a, int64_t n, int64_t k, void* stream) {
   if ((rc = enqueue_partition<U, KIND>(ctx, d, n, st, o, s)) != HPCS_OK) return rc;
   HPCS_CUDA(cudaMemcpyAsync(d, o, size_t(n) * sizeof(U), cudaMemcpyDeviceToDevice, s));
   return HPCS_OK;
-}
-
-// The k largest of in[0..n) into out[0..k), ascending (device pointers).
-template <class T, class U, int KIND>
-int topk_largest_enqueue(hpcs_ctx* ctx, const U* d, int64_t n, int64_t k, U* out, cudaStream_t s) {
-  SelectState* st = nullptr;
-  int rc;
-  if ((rc = enqueue_select<U, KIND>(ctx, d, n, n - k, s, &st)) != HPCS_OK) return rc;
-  const int64_t want = (n + SEL_NT * 4 - 1) / (SEL_NT * 4);
-  const int grid = int(want < 1 ? 1 : (want > int64_t(ctx->sms) * 2 ? int64_t(ctx->sms) * 2 : want));
-  {
-    KernelTimer kt(ctx, s, HPCS_K_TOPK);
-    topk_gather_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, k, st, out);
-    HPCS_CUDA(cudaGetLastError());
-  }
-  return enqueue_sort<U, KIND, NoValue>(ctx, out, nullptr, k, s);
 }
 
 int check_topk_args(hpcs_ctx* ctx, const void* in, const void* out, int64_t n, int64_t k) {
@@ -498,7 +440,7 @@ int hpcs_ctx_destroy(hpcs_ctx* ctx) {
   DevBuf* bufs[] = {&ctx->keys_a, &ctx->keys_b, &ctx->vals_a, &ctx->vals_b, &ctx->status0, &ctx->status1,
                     &ctx->plan,   &ctx->counts, &ctx->err_accum, &ctx->aux0, &ctx->aux1, &ctx->aux2};
   for (DevBuf* b : bufs)
-    if (b->ptr) cudaFree(b->ptr);
+    if (b->ptr && !b->borrowed) cudaFree(b->ptr);
   for (auto& t : ctx->timed) {
     cudaEventDestroy(t.a);
     cudaEventDestroy(t.b);

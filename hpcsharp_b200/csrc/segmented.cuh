@@ -1,0 +1,305 @@
+// Batched segmented LSD sort: thousands of independent arrays of mixed length and dtype in
+// one persistent launch.
+//
+// No reference counterpart (HPCsharp sorts one array per call); it is the batched form of
+// the same stable LSD sort, with identical per-array results.
+//
+// One CTA owns one segment at a time (segments are taken from a device-side queue, largest
+// first, so the long ones start early).  Because a digit histogram does not depend on the
+// order of the keys, the CTA reads its segment once to histogram every digit, then runs each
+// 8-bit pass tile by tile with running per-digit offsets: tiles of one segment are processed
+// in order by one CTA, so no look-back between CTAs is needed and every pass is one read and
+// one write (the onesweep's 36 B/key for 32-bit keys).  Segments that fit in one tile are
+// sorted entirely in shared memory: one global read, all passes in shared memory, one
+// global write.  Ranking is the sort's in-warp ranking (ordered shared atomics after the
+// lane-order probe, or the peer-mask ranking).
+#pragma once
+#include <cstdint>
+
+#include "common.cuh"
+#include "radix_kernels.cuh"
+
+namespace hpcs {
+
+// Device-resident segment descriptor.
+struct SegDesc {
+  void* keys;     // device pointer, sorted in place
+  void* scratch;  // device scratch of the same size (segments larger than one tile)
+  int64_t n;
+  int32_t dtype;  // hpcs_dtype
+  int32_t pad;
+};
+
+struct SegParams {
+  const SegDesc* segs;
+  int nsegs;
+  uint32_t* queue;  // next segment index (zeroed before each launch)
+  uint32_t* err;    // device error bits
+};
+
+template <int NT, int KPT, int MODE>
+struct SegSmem {
+  static constexpr int NW = NT / 32;
+  static constexpr int TILE_BYTES = NT * KPT * 4;  // u32 keys per tile = NT*KPT; u64 = half
+  static constexpr size_t OFF_BUF = 0;             // [2][TILE_BYTES]
+  static constexpr size_t OFF_CNT = OFF_BUF + 2 * size_t(TILE_BYTES);
+  static constexpr size_t OFF_MSK = OFF_CNT + size_t(NW) * RADIX * 4;
+  static constexpr size_t MSK_BYTES = MODE == RANK_PEER_MASK ? size_t(NW) * 2 * RADIX * 4 : 0;
+  static constexpr size_t OFF_HIST = OFF_MSK + MSK_BYTES;  // [8][256]
+  static constexpr size_t OFF_RUN = OFF_HIST + 8 * RADIX * 4;
+  static constexpr size_t OFF_LOCAL = OFF_RUN + RADIX * 4;
+  static constexpr size_t OFF_GBASE = OFF_LOCAL + RADIX * 4;
+  static constexpr size_t OFF_WSUM = OFF_GBASE + RADIX * 4;
+  static constexpr size_t OFF_SEG = OFF_WSUM + 32 * 4;
+  static constexpr size_t BYTES = OFF_SEG + 16;
+};
+
+// Ranks one tile of keys held warp-striped in registers (key i of lane l = tile position
+// w*32*KPT + i*32 + l) by digit `shift`, turns the warp counters into tile positions and
+// leaves the tile-local digit starts in s_local and the per-digit totals computable as
+// s_local[d+1]-s_local[d].  Returns each key's tile position in pos[].
+template <class U, int KIND, int NT, int KPT, int MODE>
+__device__ __forceinline__ void seg_rank_tile(const U (&key)[KPT], int tile_n, int shift, uint32_t* s_cnt,
+                                              uint32_t* s_msk, uint32_t* s_local, uint32_t* s_wsum,
+                                              uint32_t (&pos)[KPT]) {
+  using KO = KeyOrder<U, KIND>;
+  constexpr int NW = NT / 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t* cnt_w = s_cnt + warp * RADIX;
+  for (int i = lane; i < RADIX; i += 32) cnt_w[i] = 0u;
+  __syncwarp();
+  const int wbase = warp * 32 * KPT;
+#pragma unroll
+  for (int i = 0; i < KPT; i++) {
+    const bool valid = wbase + i * 32 + lane < tile_n;
+    pos[i] = rank_in_warp<MODE>(cnt_w, s_msk + warp * 2 * RADIX, KO::digit(key[i], shift), valid, i & 1, lane);
+  }
+  __syncthreads();
+  if (tid < RADIX) {
+    const int dg = tid;
+    uint32_t total = 0;
+#pragma unroll
+    for (int w = 0; w < NW; w++) total += s_cnt[w * RADIX + dg];
+    uint32_t incl = total;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    s_local[dg] = incl - total;
+    if (lane == 31) s_wsum[warp] = incl;
+  }
+  __syncthreads();
+  if (tid < RADIX) {
+    const int dg = tid;
+    uint32_t base = 0;
+#pragma unroll
+    for (int w = 0; w < RADIX / 32; w++) base += (w < warp) ? s_wsum[w] : 0u;
+    const uint32_t local = base + s_local[dg];
+    s_local[dg] = local;
+    uint32_t run = local;
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+      const uint32_t c = s_cnt[w * RADIX + dg];
+      s_cnt[w * RADIX + dg] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < KPT; i++) {
+    if (wbase + i * 32 + lane < tile_n) pos[i] += cnt_w[KO::digit(key[i], shift)];
+  }
+}
+
+// A segment that fits in one tile: one global read, every pass in shared memory, one write.
+template <class U, int KIND, int NT, int KPT, int MODE>
+__device__ void seg_sort_small(U* keys, int n, unsigned char* smem) {
+  using L = SegSmem<NT, KPT * int(sizeof(U)) / 4, MODE>;
+  constexpr int P = int(sizeof(U));
+  U* buf0 = reinterpret_cast<U*>(smem + L::OFF_BUF);
+  U* buf1 = reinterpret_cast<U*>(smem + L::OFF_BUF + L::TILE_BYTES);
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + L::OFF_CNT);
+  uint32_t* s_msk = reinterpret_cast<uint32_t*>(smem + L::OFF_MSK);
+  uint32_t* s_local = reinterpret_cast<uint32_t*>(smem + L::OFF_LOCAL);
+  uint32_t* s_wsum = reinterpret_cast<uint32_t*>(smem + L::OFF_WSUM);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wbase = warp * 32 * KPT;
+  U key[KPT];
+  uint32_t pos[KPT];
+#pragma unroll
+  for (int i = 0; i < KPT; i++) {
+    const int idx = wbase + i * 32 + lane;
+    key[i] = idx < n ? keys[idx] : U(0);
+  }
+  U* src = buf0;
+  U* dst = buf1;
+  for (int p = 0; p < P; p++) {
+    if (p > 0) {
+#pragma unroll
+      for (int i = 0; i < KPT; i++) {
+        const int idx = wbase + i * 32 + lane;
+        key[i] = idx < n ? src[idx] : U(0);
+      }
+    }
+    seg_rank_tile<U, KIND, NT, KPT, MODE>(key, n, 8 * p, s_cnt, s_msk, s_local, s_wsum, pos);
+#pragma unroll
+    for (int i = 0; i < KPT; i++)
+      if (wbase + i * 32 + lane < n) dst[pos[i]] = key[i];
+    __syncthreads();
+    U* t = src;
+    src = dst;
+    dst = t;
+  }
+  for (int i = tid; i < n; i += NT) keys[i] = src[i];
+  __syncthreads();
+}
+
+// A segment larger than one tile: histogram every digit in one read, then per pass the
+// tiles in order with running per-digit offsets (ping-pong with the segment's scratch).
+template <class U, int KIND, int NT, int KPT, int MODE>
+__device__ void seg_sort_large(U* keys, U* scratch, int64_t n, unsigned char* smem, uint32_t* err) {
+  using KO = KeyOrder<U, KIND>;
+  using L = SegSmem<NT, KPT * int(sizeof(U)) / 4, MODE>;
+  constexpr int P = int(sizeof(U));
+  constexpr int TILE = NT * KPT;
+  U* sk = reinterpret_cast<U*>(smem + L::OFF_BUF);
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + L::OFF_CNT);
+  uint32_t* s_msk = reinterpret_cast<uint32_t*>(smem + L::OFF_MSK);
+  uint32_t* s_hist = reinterpret_cast<uint32_t*>(smem + L::OFF_HIST);
+  uint32_t* s_run = reinterpret_cast<uint32_t*>(smem + L::OFF_RUN);
+  uint32_t* s_local = reinterpret_cast<uint32_t*>(smem + L::OFF_LOCAL);
+  uint32_t* s_gbase = reinterpret_cast<uint32_t*>(smem + L::OFF_GBASE);
+  uint32_t* s_wsum = reinterpret_cast<uint32_t*>(smem + L::OFF_WSUM);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  // all-digit histogram of the segment (order-independent, so one read serves every pass)
+  for (int i = tid; i < P * RADIX; i += NT) s_hist[i] = 0u;
+  __syncthreads();
+  for (int64_t i = tid; i < n; i += NT) {
+    const U o = KO::to_ordered(keys[i]);
+#pragma unroll
+    for (int d = 0; d < P; d++) atomicAdd(&s_hist[d * RADIX + (uint32_t(o >> (8 * d)) & 0xFFu)], 1u);
+  }
+  __syncthreads();
+
+  const int wbase = warp * 32 * KPT;
+  U* src = keys;
+  U* dst = scratch;
+  for (int p = 0; p < P; p++) {
+    // digit starts of this pass; a pass whose keys all share one digit is the identity
+    bool trivial = false;
+    if (tid < RADIX) {
+      const uint32_t c = s_hist[p * RADIX + tid];
+      uint32_t incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      s_run[tid] = incl - c;
+      if (lane == 31) s_wsum[warp] = incl;
+    }
+    __syncthreads();
+    if (tid < RADIX) {
+      uint32_t base = 0;
+      for (int w = 0; w < (tid >> 5); w++) base += s_wsum[w];
+      s_run[tid] += base;
+    }
+    trivial = __syncthreads_or(tid < RADIX && int64_t(s_hist[p * RADIX + tid]) == n) != 0;
+    if (trivial) continue;
+    for (int64_t tb = 0; tb < n; tb += TILE) {
+      const int tile_n = int((n - tb) < TILE ? (n - tb) : TILE);
+      U key[KPT];
+      uint32_t pos[KPT];
+#pragma unroll
+      for (int i = 0; i < KPT; i++) {
+        const int idx = wbase + i * 32 + lane;
+        key[i] = idx < tile_n ? src[tb + idx] : U(0);
+      }
+      seg_rank_tile<U, KIND, NT, KPT, MODE>(key, tile_n, 8 * p, s_cnt, s_msk, s_local, s_wsum, pos);
+#pragma unroll
+      for (int i = 0; i < KPT; i++)
+        if (wbase + i * 32 + lane < tile_n) sk[pos[i]] = key[i];
+      if (tid < RADIX) s_gbase[tid] = s_run[tid] - s_local[tid];
+      __syncthreads();
+      bool bad = false;
+      for (int s = tid; s < tile_n; s += NT) {
+        const U k = sk[s];
+        const uint32_t dpos = s_gbase[KO::digit(k, 8 * p)] + uint32_t(s);
+        if (int64_t(dpos) < n) dst[dpos] = k;
+        else bad = true;
+      }
+      if (bad) atomicOr(err, uint32_t(DERR_BOUNDS));
+      __syncthreads();
+      // advance the running offsets by this tile's digit counts
+      if (tid < RADIX) {
+        const uint32_t next = tid + 1 < RADIX ? s_local[tid + 1] : uint32_t(tile_n);
+        s_run[tid] += next - s_local[tid];
+      }
+      __syncthreads();
+    }
+    U* t = src;
+    src = dst;
+    dst = t;
+  }
+  // an odd number of executed passes leaves the result in scratch
+  if (src != keys) {
+    for (int64_t i = tid; i < n; i += NT) keys[i] = src[i];
+  }
+  __syncthreads();
+}
+
+template <int NT, int KPT, int MODE>
+__global__ void __launch_bounds__(NT, 1) segmented_sort_kernel(SegParams prm) {
+  static_assert(NT >= RADIX, "one thread per digit needed");
+  using L = SegSmem<NT, KPT, MODE>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  int* s_seg = reinterpret_cast<int*>(smem + L::OFF_SEG);
+  uint32_t* s_msk = reinterpret_cast<uint32_t*>(smem + L::OFF_MSK);
+  if (MODE == RANK_PEER_MASK)
+    for (int i = threadIdx.x; i < L::NW * 2 * RADIX; i += NT) s_msk[i] = 0u;
+  uint32_t* err = prm.err;
+  for (;;) {
+    if (threadIdx.x == 0) *s_seg = int(atomicAdd(prm.queue, 1u));
+    __syncthreads();
+    const int sidx = *s_seg;
+    __syncthreads();
+    if (sidx >= prm.nsegs) break;
+    const SegDesc sd = prm.segs[sidx];
+    if (sd.n <= 1) continue;
+    const bool small32 = sd.n <= int64_t(NT) * KPT;
+    const bool small64 = sd.n <= int64_t(NT) * (KPT / 2);
+    switch (sd.dtype) {
+      case 0:  // u32
+        if (small32) seg_sort_small<uint32_t, KIND_UNSIGNED, NT, KPT, MODE>(static_cast<uint32_t*>(sd.keys), int(sd.n), smem);
+        else seg_sort_large<uint32_t, KIND_UNSIGNED, NT, KPT, MODE>(static_cast<uint32_t*>(sd.keys), static_cast<uint32_t*>(sd.scratch), sd.n, smem, err);
+        break;
+      case 1:  // i32
+        if (small32) seg_sort_small<uint32_t, KIND_SIGNED, NT, KPT, MODE>(static_cast<uint32_t*>(sd.keys), int(sd.n), smem);
+        else seg_sort_large<uint32_t, KIND_SIGNED, NT, KPT, MODE>(static_cast<uint32_t*>(sd.keys), static_cast<uint32_t*>(sd.scratch), sd.n, smem, err);
+        break;
+      case 2:  // f32
+        if (small32) seg_sort_small<uint32_t, KIND_FLOAT, NT, KPT, MODE>(static_cast<uint32_t*>(sd.keys), int(sd.n), smem);
+        else seg_sort_large<uint32_t, KIND_FLOAT, NT, KPT, MODE>(static_cast<uint32_t*>(sd.keys), static_cast<uint32_t*>(sd.scratch), sd.n, smem, err);
+        break;
+      case 3:  // u64
+        if (small64) seg_sort_small<uint64_t, KIND_UNSIGNED, NT, KPT / 2, MODE>(static_cast<uint64_t*>(sd.keys), int(sd.n), smem);
+        else seg_sort_large<uint64_t, KIND_UNSIGNED, NT, KPT / 2, MODE>(static_cast<uint64_t*>(sd.keys), static_cast<uint64_t*>(sd.scratch), sd.n, smem, err);
+        break;
+      case 4:  // i64
+        if (small64) seg_sort_small<uint64_t, KIND_SIGNED, NT, KPT / 2, MODE>(static_cast<uint64_t*>(sd.keys), int(sd.n), smem);
+        else seg_sort_large<uint64_t, KIND_SIGNED, NT, KPT / 2, MODE>(static_cast<uint64_t*>(sd.keys), static_cast<uint64_t*>(sd.scratch), sd.n, smem, err);
+        break;
+      case 5:  // f64
+        if (small64) seg_sort_small<uint64_t, KIND_FLOAT, NT, KPT / 2, MODE>(static_cast<uint64_t*>(sd.keys), int(sd.n), smem);
+        else seg_sort_large<uint64_t, KIND_FLOAT, NT, KPT / 2, MODE>(static_cast<uint64_t*>(sd.keys), static_cast<uint64_t*>(sd.scratch), sd.n, smem, err);
+        break;
+      default:
+        if (threadIdx.x == 0) atomicOr(err, uint32_t(DERR_BOUNDS));
+        break;
+    }
+  }
+}
+
+}  // namespace hpcs

@@ -25,10 +25,12 @@ int cuda_fail(cudaError_t e, const char* what);
     if (e_ != cudaSuccess) return ::hpcs::cuda_fail(e_, #call); \
   } while (0)
 
-// Grow-only device buffer owned by a context.
+// Grow-only device buffer owned by a context.  A borrowed buffer is a slice of memory that
+// someone else owns (the serving arena): it is never grown or freed by the context.
 struct DevBuf {
   void* ptr = nullptr;
   size_t bytes = 0;
+  bool borrowed = false;
 };
 
 }  // namespace hpcs

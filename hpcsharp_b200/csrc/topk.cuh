@@ -35,7 +35,7 @@ struct SelectState {
   uint32_t hist[256];
 };
 
-__global__ void select_init_kernel(SelectState* st, int64_t rank) {
+static __global__ void select_init_kernel(SelectState* st, int64_t rank) {
   const int tid = threadIdx.x;
   if (tid == 0) {
     st->prefix = 0;
@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(PART_NT) partition_count_kernel(const U* __res
 }
 
 // One block: tile_counts[t][c] -> exclusive start of tile t's class-c keys in the output.
-__global__ void partition_scan_kernel(uint32_t* tile_counts, int64_t tiles, const SelectState* st, int64_t n) {
+static __global__ void partition_scan_kernel(uint32_t* tile_counts, int64_t tiles, const SelectState* st, int64_t n) {
   __shared__ int64_t carry[3];
   __shared__ int64_t wsum[3][32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;  // 1024 threads

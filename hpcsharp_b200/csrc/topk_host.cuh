@@ -1,0 +1,70 @@
+// Host-side enqueue sequences of the radix select / top-k kernels (topk.cuh), shared by the
+// C ABI and the serving runtime.  Scratch comes from the context's buffers (aux0: candidate
+// keys, aux1: SelectState, aux2: partition tile counts), which the serving runtime binds to
+// slices of its arena.
+#pragma once
+#include "sort_host.cuh"
+#include "topk.cuh"
+
+namespace hpcs {
+
+// Radix select of the key of 0-based rank `rank` among n keys at device pointer d.  Leaves
+// the SelectState in ctx->aux1 (prefix = the ordered bits of the selected key, less/eq counts).
+template <class U, int KIND>
+inline int enqueue_select(hpcs_ctx* ctx, const U* d, int64_t n, int64_t rank, cudaStream_t s, SelectState** out) {
+  constexpr int BITS = int(sizeof(U) * 8);
+  constexpr int LEVELS = BITS / 8;
+  int rc;
+  if ((rc = ensure(ctx, ctx->aux1, sizeof(SelectState))) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->aux0, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
+  SelectState* st = static_cast<SelectState*>(ctx->aux1.ptr);
+  U* cand = static_cast<U*>(ctx->aux0.ptr);
+  KernelTimer kt(ctx, s, HPCS_K_TOPK);
+  select_init_kernel<<<1, 256, 0, s>>>(st, rank);
+  const int64_t want = (n + SEL_NT * 4 - 1) / (SEL_NT * 4);
+  const int grid = int(want < 1 ? 1 : (want > int64_t(ctx->sms) * 2 ? int64_t(ctx->sms) * 2 : want));
+  select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, nullptr, n, st, BITS - 8);
+  select_pick_kernel<U><<<1, 256, 0, s>>>(st, BITS - 8, LEVELS == 1);
+  select_compact_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, cand, st);
+  for (int l = 1; l < LEVELS; l++) {
+    const int shift = BITS - 8 * (l + 1);
+    select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(cand, &st->cand_count, 0, st, shift);
+    select_pick_kernel<U><<<1, 256, 0, s>>>(st, shift, l == LEVELS - 1);
+  }
+  HPCS_CUDA(cudaGetLastError());
+  *out = st;
+  return HPCS_OK;
+}
+
+// Stable three-way partition of d[0..n) around the selected key into out.
+template <class U, int KIND>
+inline int enqueue_partition(hpcs_ctx* ctx, const U* d, int64_t n, SelectState* st, U* out, cudaStream_t s) {
+  const int64_t tiles = (n + PART_TILE - 1) / PART_TILE;
+  int rc;
+  if ((rc = ensure(ctx, ctx->aux2, size_t(tiles) * 3 * 4)) != HPCS_OK) return rc;
+  uint32_t* tc = static_cast<uint32_t*>(ctx->aux2.ptr);
+  KernelTimer kt(ctx, s, HPCS_K_TOPK);
+  partition_count_kernel<U, KIND><<<int(tiles), PART_NT, 0, s>>>(d, n, st, tc);
+  partition_scan_kernel<<<1, 1024, 0, s>>>(tc, tiles, st, n);
+  partition_scatter_kernel<U, KIND><<<int(tiles), PART_NT, 0, s>>>(d, n, st, tc, out);
+  HPCS_CUDA(cudaGetLastError());
+  return HPCS_OK;
+}
+
+// The k largest of in[0..n) into out[0..k), ascending (device pointers).
+template <class T, class U, int KIND>
+inline int topk_largest_enqueue(hpcs_ctx* ctx, const U* d, int64_t n, int64_t k, U* out, cudaStream_t s) {
+  SelectState* st = nullptr;
+  int rc;
+  if ((rc = enqueue_select<U, KIND>(ctx, d, n, n - k, s, &st)) != HPCS_OK) return rc;
+  const int64_t want = (n + SEL_NT * 4 - 1) / (SEL_NT * 4);
+  const int grid = int(want < 1 ? 1 : (want > int64_t(ctx->sms) * 2 ? int64_t(ctx->sms) * 2 : want));
+  {
+    KernelTimer kt(ctx, s, HPCS_K_TOPK);
+    topk_gather_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, k, st, out);
+    HPCS_CUDA(cudaGetLastError());
+  }
+  return enqueue_sort<U, KIND, NoValue>(ctx, out, nullptr, k, s);
+}
+
+}  // namespace hpcs

@@ -72,6 +72,30 @@ class HpcsConfig(C.Structure):
 KCLASS = {"histogram": 0, "onesweep": 1, "finalize": 2, "topk": 3, "segmented": 4}
 
 
+class HpcsSegment(C.Structure):
+    _fields_ = [("keys", C.c_void_p), ("n", C.c_int64), ("dtype", C.c_int32), ("reserved", C.c_int32)]
+
+
+class HpcsRequest(C.Structure):
+    _fields_ = [("op", C.c_int32), ("dtype", C.c_int32), ("input", C.c_void_p), ("output", C.c_void_p),
+                ("n", C.c_int64), ("k", C.c_int64)]
+
+
+class HpcsRequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("coalesced", C.c_int32), ("submit_ns", C.c_int64),
+                ("admit_ns", C.c_int64), ("done_ns", C.c_int64)]
+
+
+class HpcsServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("slots", C.c_int32), ("hbm_budget_bytes", C.c_int64),
+                ("coalesce_max_keys", C.c_int64), ("coalesce_max_requests", C.c_int32), ("reserved", C.c_int32 * 5)]
+
+
+class HpcsServerCounters(C.Structure):
+    _fields_ = [(f, C.c_int64) for f in ("completed", "keys", "batches", "coalesced", "pending", "arena_bytes",
+                                         "arena_used", "arena_peak")]
+
+
 class HpcsProfile(C.Structure):
     _fields_ = [("launches", C.c_int64 * 8), ("total_ms", C.c_double * 8)]
 
@@ -113,6 +137,17 @@ def _declare(lib) -> None:
     lib.hpcs_ctx_profile_enable.argtypes = [P, I32]
     lib.hpcs_ctx_profile_read.argtypes = [P, C.POINTER(HpcsProfile)]
     lib.hpcs_ctx_trace_tiles.argtypes = [P, P, I32, I32]
+    lib.hpcs_sort_segmented_dev.argtypes = [P, C.POINTER(HpcsSegment), I64, P]
+    lib.hpcs_segplan_create.argtypes = [P, C.POINTER(HpcsSegment), I64, C.POINTER(P)]
+    lib.hpcs_segplan_execute.argtypes = [P, P]
+    lib.hpcs_segplan_destroy.argtypes = [P]
+    lib.hpcs_server_config_default.argtypes = [C.POINTER(HpcsServerConfig)]
+    lib.hpcs_server_config_default.restype = None
+    lib.hpcs_server_create.argtypes = [C.POINTER(HpcsServerConfig), C.POINTER(P)]
+    lib.hpcs_server_submit.argtypes = [P, C.POINTER(HpcsRequest), C.POINTER(C.c_uint64)]
+    lib.hpcs_server_wait.argtypes = [P, C.c_uint64, I64, C.POINTER(HpcsRequestInfo)]
+    lib.hpcs_server_stats.argtypes = [P, C.POINTER(HpcsServerCounters)]
+    lib.hpcs_server_destroy.argtypes = [P]
 
 
 def load():
@@ -278,10 +313,56 @@ class Context:
         check(getattr(self.lib, f"hpcs_topk_largest_{name}_dev")(self.handle, _ptr(t), t.numel(), k, _ptr(out),
                                                                  stream))
 
+    def sort_segmented_dev(self, segments, stream: int | None = None) -> None:
+        """segments: list of (device tensor or (ptr, n), dtype name).  Sorted in place."""
+        arr = make_segments(segments)
+        check(self.lib.hpcs_sort_segmented_dev(self.handle, arr, len(arr), stream))
+
+    def segplan(self, segments) -> "SegPlan":
+        return SegPlan(self, segments)
+
     def histogram_dev(self, t, counts, dtype: str | None = None, stream: int | None = None) -> None:
         name = dtype or _torch_dtype_name(t)
         check(self.lib.hpcs_histogram_byte_components_dev(self.handle, DTYPES[name], _ptr(t), t.numel(),
                                                           _ptr(counts), stream))
+
+
+def make_segments(segments):
+    arr = (HpcsSegment * len(segments))()
+    for i, (t, dt) in enumerate(segments):
+        if isinstance(t, tuple):
+            ptr, n = t
+        else:
+            ptr, n = _ptr(t), t.numel()
+        arr[i].keys = ptr
+        arr[i].n = n
+        arr[i].dtype = DTYPES[dt]
+    return arr
+
+
+class SegPlan:
+    """A batched segmented sort captured once (device-resident descriptors + CUDA graph)."""
+
+    def __init__(self, ctx: "Context", segments):
+        self.ctx = ctx
+        arr = make_segments(segments)
+        h = C.c_void_p()
+        check(ctx.lib.hpcs_segplan_create(ctx.handle, arr, len(arr), C.byref(h)))
+        self.handle = h
+
+    def execute(self, stream: int | None = None) -> None:
+        check(self.ctx.lib.hpcs_segplan_execute(self.handle, stream))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.ctx.lib.hpcs_segplan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _torch_dtype_name(t) -> str:
@@ -295,6 +376,56 @@ def _torch_dtype_name(t) -> str:
     if t.dtype not in m:
         raise TypeError(f"unsupported tensor dtype {t.dtype}; pass dtype=")
     return m[t.dtype]
+
+
+OPS = {"sort": 0, "topk": 1}
+
+
+class Server:
+    """Continuous-batching sort / top-k server (hpcs_server_* in the C ABI)."""
+
+    def __init__(self, device: int = 0, *, slots: int = 4, hbm_budget_bytes: int = 16 << 30,
+                 coalesce_max_keys: int = 1 << 17, coalesce_max_requests: int = 4096):
+        self.lib = load()
+        cfg = HpcsServerConfig()
+        self.lib.hpcs_server_config_default(C.byref(cfg))
+        cfg.device, cfg.slots, cfg.hbm_budget_bytes = device, slots, hbm_budget_bytes
+        cfg.coalesce_max_keys, cfg.coalesce_max_requests = coalesce_max_keys, coalesce_max_requests
+        h = C.c_void_p()
+        check(self.lib.hpcs_server_create(C.byref(cfg), C.byref(h)))
+        self.handle = h
+
+    def submit(self, op: str, keys: np.ndarray, out: np.ndarray, k: int = 0) -> int:
+        """Queues a request; keys/out must stay alive until wait() returns for its ticket."""
+        r = HpcsRequest()
+        r.op, r.dtype = OPS[op], DTYPES[dtype_name(keys.dtype)]
+        r.input, r.output, r.n, r.k = keys.ctypes.data, out.ctypes.data, keys.size, k
+        t = C.c_uint64()
+        check(self.lib.hpcs_server_submit(self.handle, C.byref(r), C.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int, timeout_ns: int = 0) -> dict:
+        info = HpcsRequestInfo()
+        status = self.lib.hpcs_server_wait(self.handle, ticket, timeout_ns, C.byref(info))
+        check(status)
+        return {"coalesced": bool(info.coalesced), "submit_ns": info.submit_ns, "admit_ns": info.admit_ns,
+                "done_ns": info.done_ns}
+
+    def stats(self) -> dict:
+        c = HpcsServerCounters()
+        check(self.lib.hpcs_server_stats(self.handle, C.byref(c)))
+        return {f: getattr(c, f) for f, _ in HpcsServerCounters._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.hpcs_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 _default_ctx: Context | None = None

@@ -179,6 +179,29 @@ int hpcs_histogram_byte_components_f64(hpcs_ctx* ctx, const double* a, int64_t l
 int hpcs_histogram_byte_components_dev(hpcs_ctx* ctx, int dtype, const void* a, int64_t n, uint32_t* counts,
                                        void* stream);
 
+/* ---- batched segmented sort ------------------------------------------------------------
+ * No reference counterpart (HPCsharp sorts one array per call): many independent arrays of
+ * mixed length and dtype sorted in one persistent launch, each with exactly the plain sort's
+ * result (stable, ascending, same order transforms).  Keys are device pointers, sorted in
+ * place; each array's n <= HPCS_MAX_KEYS. */
+typedef struct hpcs_segment {
+  void* keys;      /* device pointer */
+  int64_t n;
+  int32_t dtype;   /* hpcs_dtype */
+  int32_t reserved;
+} hpcs_segment;
+
+/* One-shot: uploads the descriptors and sorts on `stream`. */
+int hpcs_sort_segmented_dev(hpcs_ctx* ctx, const hpcs_segment* segs, int64_t nsegs, void* stream);
+
+/* Reusable plan: descriptors stay on the device (largest array first), scratch is reserved,
+ * and the launch is captured in a CUDA graph; hpcs_segplan_execute replays it (sorting
+ * whatever the same arrays hold at that time). */
+typedef struct hpcs_segplan hpcs_segplan;
+int hpcs_segplan_create(hpcs_ctx* ctx, const hpcs_segment* segs, int64_t nsegs, hpcs_segplan** out);
+int hpcs_segplan_execute(hpcs_segplan* plan, void* stream);
+int hpcs_segplan_destroy(hpcs_segplan* plan);
+
 /* ---- radix top-k ---------------------------------------------------------------------
  * Algorithm.SelectTopK(this uint[] a, int k) SelectionTopKRadix.cs:160-171 (and the
  * (a, start, length, k) form :142-153 via a pointer offset): afterwards a[k] is the k-th
@@ -213,6 +236,60 @@ int hpcs_topk_largest_f32_dev(hpcs_ctx* ctx, const float* in, int64_t n, int64_t
 int hpcs_topk_largest_u64_dev(hpcs_ctx* ctx, const uint64_t* in, int64_t n, int64_t k, uint64_t* out, void* stream);
 int hpcs_topk_largest_i64_dev(hpcs_ctx* ctx, const int64_t* in, int64_t n, int64_t k, int64_t* out, void* stream);
 int hpcs_topk_largest_f64_dev(hpcs_ctx* ctx, const double* in, int64_t n, int64_t k, double* out, void* stream);
+
+/* ---- serving: continuous batching of sort and top-k requests ---------------------------
+ * No reference counterpart (HPCsharp is a synchronous library).  Requests of any size and
+ * dtype are submitted at any time from any thread; a scheduler thread admits each one as
+ * soon as its keys and scratch fit in the server's HBM budget (a device arena reserved at
+ * creation) and an execution slot (a CUDA stream) is free, and runs admitted requests
+ * concurrently; requests of at most coalesce_max_keys keys are gathered into one batched
+ * segmented-sort launch.  Each result equals the plain entry point's result on the same input
+ * (sort: hpcs_sort_<t>; top-k: hpcs_topk_largest_<t>).  Host buffers in pinned memory let
+ * the copies overlap with other requests' kernels. */
+typedef enum hpcs_op { HPCS_OP_SORT = 0, HPCS_OP_TOPK = 1 } hpcs_op;
+
+typedef struct hpcs_request {
+  int32_t op;          /* hpcs_op */
+  int32_t dtype;       /* hpcs_dtype */
+  const void* input;   /* host keys, n of them (read after submit, until the request is done) */
+  void* output;        /* host: n sorted keys (sort) or the k largest ascending (top-k) */
+  int64_t n;
+  int64_t k;           /* top-k only, 0 <= k <= n */
+} hpcs_request;
+
+typedef struct hpcs_request_info {
+  int32_t status;      /* hpcs_status of the request */
+  int32_t coalesced;   /* 1 if it ran inside a batched segmented launch */
+  int64_t submit_ns;   /* steady clock */
+  int64_t admit_ns;
+  int64_t done_ns;
+} hpcs_request_info;
+
+typedef struct hpcs_server_config {
+  int32_t device;
+  int32_t slots;                  /* concurrent large requests (CUDA streams), default 4 */
+  int64_t hbm_budget_bytes;       /* device arena for keys and scratch, default 64 GiB */
+  int64_t coalesce_max_keys;      /* requests up to this size are batched, default 131072 */
+  int32_t coalesce_max_requests;  /* per batched launch, default 4096 */
+  int32_t reserved[5];
+} hpcs_server_config;
+
+typedef struct hpcs_server_counters {
+  int64_t completed, keys, batches, coalesced, pending;
+  int64_t arena_bytes, arena_used, arena_peak;
+} hpcs_server_counters;
+
+typedef struct hpcs_server hpcs_server;
+void hpcs_server_config_default(hpcs_server_config* cfg);
+int hpcs_server_create(const hpcs_server_config* cfg, hpcs_server** out);
+/* HPCS_ERR_OOM: the request can never fit the HBM budget. */
+int hpcs_server_submit(hpcs_server* server, const hpcs_request* req, uint64_t* ticket);
+/* Blocks until the request is done (timeout_ns <= 0: no limit; HPCS_ERR_BUSY on timeout),
+ * fills info and returns the request's status; the ticket is then released. */
+int hpcs_server_wait(hpcs_server* server, uint64_t ticket, int64_t timeout_ns, hpcs_request_info* info);
+int hpcs_server_stats(hpcs_server* server, hpcs_server_counters* stats);
+/* Finishes every submitted request, then frees the server. */
+int hpcs_server_destroy(hpcs_server* server);
 
 /* ---- uint32 device sort that allocates nothing --------------------------------------
  * No counterpart in the reference (HPCsharp allocates managed arrays per call).  For callers

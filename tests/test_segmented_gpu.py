@@ -1,0 +1,120 @@
+"""Batched segmented sort: every array of a mixed batch equals the oracle's sort of that array
+alone (bit for bit), for all dtypes and lengths around the in-shared-memory / tiled threshold,
+through the one-shot call and the graph-captured plan."""
+import numpy as np
+import pytest
+
+from hpcsharp_b200 import datagen, native
+from tests.gpu_util import from_dev, to_dev
+
+pytestmark = pytest.mark.gpu
+
+LENGTHS = [0, 1, 2, 31, 32, 33, 255, 4095, 4096, 4097, 8191, 8192, 8193, 20_000, 65_536, 300_001]
+DT = ["u32", "i32", "f32", "u64", "i64", "f64"]
+
+
+def make_batch(seed, lengths=LENGTHS, dtypes=DT):
+    rng = np.random.default_rng(seed)
+    host = []
+    for i, n in enumerate(lengths):
+        dt = dtypes[rng.integers(len(dtypes))] if len(dtypes) > 1 else dtypes[0]
+        host.append((datagen.by_name(dt, n, seed=seed * 1000 + i), dt))
+    return host
+
+
+def oracle_sorted(orc, a):
+    s = a.copy()
+    orc.sort_radix_lsd(s)
+    return s
+
+
+def check(host, devs, orc):
+    for (a, dt), t in zip(host, devs):
+        got = from_dev(t, a.dtype) if a.size else a
+        want = oracle_sorted(orc, a)
+        assert np.array_equal(got.view(np.uint8), want.view(np.uint8)), (dt, a.size)
+
+
+@pytest.mark.parametrize("dt", DT)
+def test_single_dtype_batch(ctx, orc, dt):
+    import torch
+
+    host = make_batch(11, dtypes=[dt])
+    devs = [to_dev(a) if a.size else torch.empty(0, device="cuda") for a, _ in host]
+    ctx.sort_segmented_dev([(t, d) for t, (_, d) in zip(devs, host)],
+                           stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    check(host, devs, orc)
+
+
+def test_mixed_batch_many_small(ctx, orc):
+    import torch
+
+    rng = np.random.default_rng(5)
+    lengths = list((32 * 2 ** rng.uniform(0, 13, size=700)).astype(np.int64))
+    host = make_batch(7, lengths=lengths)
+    devs = [to_dev(a) for a, _ in host]
+    ctx.sort_segmented_dev([(t, d) for t, (_, d) in zip(devs, host)],
+                           stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    check(host, devs, orc)
+
+
+def test_plan_graph_replays(ctx, orc):
+    import torch
+
+    host = make_batch(21)
+    devs = [to_dev(a) if a.size else torch.empty(0, device="cuda") for a, _ in host]
+    plan = ctx.segplan([(t, d) for t, (_, d) in zip(devs, host)])
+    try:
+        s = torch.cuda.current_stream().cuda_stream
+        plan.execute(s)
+        torch.cuda.synchronize()
+        ctx.synchronize()
+        check(host, devs, orc)
+        # new data in the same arrays, same graph
+        host2 = [(datagen.by_name(d, a.size, seed=999 + i), d) for i, (a, d) in enumerate(host)]
+        for t, (a, _) in zip(devs, host2):
+            if a.size:
+                t.copy_(to_dev(a))
+        torch.cuda.synchronize()
+        plan.execute(s)
+        torch.cuda.synchronize()
+        ctx.synchronize()
+        check(host2, devs, orc)
+    finally:
+        plan.close()
+
+
+def test_segmented_equals_plain_sort(ctx):
+    """The batched result equals the plain per-array entry point's result."""
+    import torch
+
+    host = make_batch(33, lengths=[5000, 9000, 123_457, 1_000_003])
+    a_dev = [to_dev(a) for a, _ in host]
+    b_dev = [to_dev(a) for a, _ in host]
+    s = torch.cuda.current_stream().cuda_stream
+    ctx.sort_segmented_dev([(t, d) for t, (_, d) in zip(a_dev, host)], stream=s)
+    for t, (_, d) in zip(b_dev, host):
+        ctx.sort_dev(t, dtype=d, stream=s)
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    for x, y in zip(a_dev, b_dev):
+        assert torch.equal(x, y)
+
+
+def test_segment_errors(ctx):
+    import ctypes as C
+
+    lib = native.load()
+    arr = (native.HpcsSegment * 1)()
+    arr[0].keys = None
+    arr[0].n = 10
+    arr[0].dtype = 0
+    assert lib.hpcs_sort_segmented_dev(ctx.handle, arr, 1, None) == native.HPCS_ERR_NULL
+    arr[0].keys = 16
+    arr[0].dtype = 9
+    assert lib.hpcs_sort_segmented_dev(ctx.handle, arr, 1, None) == native.HPCS_ERR_UNSUPPORTED
+    assert lib.hpcs_sort_segmented_dev(ctx.handle, None, 0, None) == native.HPCS_OK
