@@ -239,7 +239,7 @@ def run_reference(args, rank: int, world: int):
 def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
 
-    from hpcsharp_b200 import native
+    from hpcsharp_b200 import native, replicas
 
     dev = local_rank
     torch.cuda.set_device(dev)
@@ -297,15 +297,13 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     prof = ctx.profile_read()
     ctx.profile(False)
     total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    total_ms = replicas.max_over_ranks(total_ms, device=f"cuda:{dev}")
     if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
     torch.cuda.synchronize()
     clk = clocks.stop()
 
-    value = n * args.steps * world / (total_ms / 1e3) / 1e9
+    value = replicas.weak_scaling_gkeys(n, args.steps, world, total_ms)
     ms_per_step = total_ms / args.steps
 
     # roofline of the dominant kernel (the onesweep digit pass): algorithmic bytes per
@@ -344,10 +342,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             t0 = time.perf_counter()
             native.check(fn(ctx.handle, pn.ctypes.data, n))
             tot += time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([tot], device=f"cuda:{dev}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            tot = float(t.item())
+        tot = replicas.max_over_ranks(tot, device=f"cuda:{dev}")
         e2e = {"value": round(n * ksteps * world / tot / 1e9, 4), "unit": UNIT,
                "h2d_bytes_per_step": n * w, "d2h_bytes_per_step": n * w, "steps": ksteps,
                "ms_per_step": round(tot / ksteps * 1e3, 3), "api": f"hpcs_sort_{dtype} (host array, pinned)"}

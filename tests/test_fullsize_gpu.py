@@ -1,0 +1,70 @@
+"""Full-size workloads (the plain-sort-at-scale and pairs configurations) checked through
+size-independent properties on the GPU: the output is in the reference's key order, it is a
+permutation of the input (order-independent checksums), and for key+index pairs every item
+points at its key in the input and equal keys keep their input order (stability).  The
+bit-exact oracle comparisons run at smaller sizes in the other test files."""
+import numpy as np
+import pytest
+
+from hpcsharp_b200 import datagen, native
+from tests.gpu_util import checksum_dev, is_sorted_dev, ordered_i64, to_dev
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+PLAIN = [
+    ("u32", 1 << 28, lambda n: datagen.u32_uniform(n, 1)),
+    ("i32", 1 << 28, lambda n: datagen.i32_normal(n, 1)),
+    ("f32", 1 << 28, lambda n: datagen.f32_normal_special(n, 1)),
+    ("u64", 1 << 27, lambda n: datagen.u64_uniform(n, 1)),
+    ("u64", 1 << 27, lambda n: datagen.u64_and3(n, 1)),
+]
+
+
+@pytest.mark.parametrize("dt,n,gen", PLAIN, ids=["u32_256M", "i32_normal_256M", "f32_specials_256M",
+                                                 "u64_uniform_128M", "u64_and3_128M"])
+def test_plain_sort_at_scale(ctx, dt, n, gen):
+    import torch
+
+    a = gen(n)
+    t = to_dev(a)
+    before = checksum_dev(t)
+    ctx.sort_dev(t, dtype=dt, stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    assert is_sorted_dev(t, dt)
+    assert checksum_dev(t) == before
+    del t
+    torch.cuda.empty_cache()
+
+
+PAIRS = [
+    ("u64", 200_000_000, lambda n: datagen.u64_zipf(n, 1)),
+    ("f64", 100_000_000, lambda n: datagen.f64_normal(n, 1)),
+]
+
+
+@pytest.mark.parametrize("dt,n,gen", PAIRS, ids=["u64_zipf_200M_pairs", "f64_normal_100M_pairs"])
+def test_pairs_at_scale(ctx, dt, n, gen):
+    import torch
+
+    a = gen(n)
+    keys = to_dev(a)
+    orig = keys.clone()
+    items = torch.arange(n, dtype=torch.int32, device="cuda")
+    ctx.sort_pairs_dev(keys, items, dtype=dt, stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    assert is_sorted_dev(keys, dt)
+    idx = items.to(torch.int64)
+    # items are a permutation of 0..n-1 and each points at its key in the input
+    assert int(idx.min()) == 0 and int(idx.max()) == n - 1
+    assert int(idx.sum()) == n * (n - 1) // 2
+    assert torch.equal(orig[idx], keys)
+    # stability: equal keys keep increasing input positions
+    o = ordered_i64(keys, dt)
+    same = o[1:] == o[:-1]
+    assert bool((idx[1:][same] > idx[:-1][same]).all())
+    if dt == "u64":
+        assert int(same.sum()) > n // 2  # Zipf duplicates are heavy
+    del keys, orig, items, idx, o, same
+    torch.cuda.empty_cache()
