@@ -56,6 +56,8 @@ def parse():
                     help="plain: the 2^28-key sort (headline); batched: 65,536 mixed arrays; "
                          "served: Poisson sort/top-k requests swept to saturation")
     ap.add_argument("--requests", type=int, default=120, help="served: requests per arrival rate")
+    ap.add_argument("--loads", default="0.25,0.5,1,2,4,8,16",
+                    help="served: offered loads, as multiples of the plain form's capacity")
     ap.add_argument("--literal", action="store_true",
                     help="batched: the literal length distribution (~6.6 G keys) instead of ~250 M")
     return ap.parse_args()
@@ -528,7 +530,7 @@ def run_served(args, rank: int, world: int, local_rank: int, emit: bool = True):
         server.wait(server.submit(reqs[i][0], inputs[i], outs_served[i], reqs[i][3]))
 
     points = []
-    for load in (0.25, 0.5, 1.0, 2.0, 4.0):
+    for load in (float(x) for x in args.loads.split(",")):
         rate = load / mean_service  # requests per second
         arrivals = np.cumsum(gaps) / rate
         # served: a client thread submits at the arrival times
