@@ -51,6 +51,37 @@ struct KeyOrder {
   }
 };
 
+// Digit of one pass with the order transform folded in: one byte permute (plus the sign
+// mask for floats) instead of the full to_ordered + shift + mask.  Only the byte the pass
+// reads is transformed: signed keys flip bit 7 of the top byte, floats flip every bit of a
+// negative key and the sign bit of a positive one.
+template <class U, int KIND>
+struct Digit;
+template <int KIND>
+struct Digit<uint32_t, KIND> {
+  uint32_t sel;
+  __device__ __forceinline__ explicit Digit(int shift) : sel(0x4440u | uint32_t(shift >> 3)) {}
+  __device__ __forceinline__ uint32_t operator()(uint32_t x) const {
+    if (KIND == KIND_SIGNED) x ^= 0x80000000u;
+    if (KIND == KIND_FLOAT) x ^= uint32_t(int32_t(x) >> 31) | 0x80000000u;
+    return __byte_perm(x, 0u, sel);
+  }
+};
+template <int KIND>
+struct Digit<uint64_t, KIND> {
+  uint32_t sel, top;
+  bool hi_word;
+  __device__ __forceinline__ explicit Digit(int shift)
+      : sel(0x4440u | uint32_t((shift >> 3) & 3)), top(shift >= 32 ? 0x80000000u : 0u), hi_word(shift >= 32) {}
+  __device__ __forceinline__ uint32_t operator()(uint64_t x) const {
+    const uint32_t hi = uint32_t(x >> 32);
+    uint32_t w = hi_word ? hi : uint32_t(x);
+    if (KIND == KIND_SIGNED) w ^= top;
+    if (KIND == KIND_FLOAT) w ^= uint32_t(int32_t(hi) >> 31) | top;
+    return __byte_perm(w, 0u, sel);
+  }
+};
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }

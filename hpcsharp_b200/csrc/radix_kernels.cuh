@@ -58,7 +58,9 @@ struct SortPlan {
   int32_t final_sel;                      // buffer holding the result (0 = A)
   uint32_t done_blocks;
   uint32_t error;                         // DeviceError bits
-  uint32_t pad;
+  uint32_t idle_flag;                     // never written: the wait-timeout test hook spins on it
+  int32_t exec_idx[MAX_PASSES];           // 0, 1, 2, ... over the executed passes
+  int32_t next_shift[MAX_PASSES];         // bit shift of the next executed pass's digit, -1 if none
 };
 
 struct SortArgs {
@@ -80,6 +82,13 @@ struct SortArgs {
   uint64_t* trace;
   int trace_pass;
   int trace_capacity;  // tiles
+  // Chunked passes (chunk_hist != null): the keys are cut into `chunks` ranges of
+  // chunk_keys keys (a whole number of tiles); CTA j of every kernel owns range j.
+  uint32_t* chunk_hist;   // [chunks][P][256] digit counts of each input range (K1)
+  uint32_t* ctab;         // [3][chunks][256] per-range counts of the next executed digit
+  int chunks;
+  uint32_t chunk_keys;
+  uint32_t chunk_magic;   // ceil(2^32 / chunk_keys): range of position p = umulhi(p, magic) (-1)
 };
 constexpr int TRACE_WORDS = 7;
 
@@ -129,12 +138,23 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
     }
   };
 
+  // Grid-stride over all vectors, or (chunked) CTA j over the vectors of key range j.
+  const bool chunked = args.chunk_hist != nullptr;
   const int64_t nvec = n / VEC;
   const uint4* vkeys = reinterpret_cast<const uint4*>(keys);
-  const int64_t stride = int64_t(gridDim.x) * NT;
+  int64_t vend = nvec, stride = int64_t(gridDim.x) * NT;
   int64_t i = int64_t(blockIdx.x) * NT + tid;
+  bool owns_tail = blockIdx.x == 0;
+  if (chunked) {
+    const int64_t lo = int64_t(blockIdx.x) * args.chunk_keys;  // a multiple of VEC
+    const int64_t hi = lo + args.chunk_keys < n ? lo + args.chunk_keys : n;
+    i = lo / VEC + tid;
+    vend = hi / VEC;
+    stride = NT;
+    owns_tail = hi == n;
+  }
   // 4 vectors in flight per thread per iteration
-  for (; i + 3 * stride < nvec; i += 4 * stride) {
+  for (; i + 3 * stride < vend; i += 4 * stride) {
     uint4 v[4];
 #pragma unroll
     for (int u = 0; u < 4; u++) v[u] = ldg_stream_v4(vkeys + i + u * stride);
@@ -145,33 +165,41 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
       for (int j = 0; j < VEC; j++) count_key(e[j]);
     }
   }
-  for (; i < nvec; i += stride) {
+  for (; i < vend; i += stride) {
     const uint4 v = ldg_stream_v4(vkeys + i);
     const U* e = reinterpret_cast<const U*>(&v);
 #pragma unroll
     for (int j = 0; j < VEC; j++) count_key(e[j]);
   }
   // ragged tail (fewer than VEC keys)
-  if (blockIdx.x == 0 && tid < VEC) {
+  if (owns_tail && tid < VEC) {
     const int64_t t = nvec * VEC + tid;
     if (t < n) count_key(keys[t]);
   }
   __syncthreads();
-  // fold the copies (rotated start so a warp's reads hit distinct banks) into the output
+  // fold the copies (rotated start so a warp's reads hit distinct banks) into the output,
+  // and (chunked) into this range's row of per-range counts
+  uint32_t* crow = chunked ? args.chunk_hist + int64_t(blockIdx.x) * P * RADIX : nullptr;
   for (int j = tid; j < P * RADIX; j += NT) {
     uint32_t c = 0;
 #pragma unroll 8
     for (int q = 0; q < COPIES; q++) c += sh[j * COPIES + ((q + lane) & (COPIES - 1))];
     if (c) atomicAdd(hist_out + j, c);
+    if (chunked) crow[j] = c;
   }
 
   if (!make_plan) return;
 
-  // Zero the first look-back buffer for the first executed pass, and the tile counters.
-  {
+  if (chunked) {
+    // the first executed pass adds its next-digit counts into table 1
+    uint32_t* t1 = args.ctab + (int64_t(args.chunks) + blockIdx.x) * RADIX;
+    for (int j = tid; j < RADIX; j += NT) t1[j] = 0;
+  } else {
+    // Zero the first look-back buffer for the first executed pass.
     uint32_t* s0 = args.status[0];
     const int64_t words = int64_t(args.num_tiles) * RADIX;
-    for (int64_t w = int64_t(blockIdx.x) * NT + tid; w < words; w += stride) s0[w] = 0;
+    const int64_t gstride = int64_t(gridDim.x) * NT;
+    for (int64_t w = int64_t(blockIdx.x) * NT + tid; w < words; w += gstride) s0[w] = 0;
   }
   // Last-block-done: the final CTA builds the plan.
   __threadfence();
@@ -210,9 +238,11 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
     __syncthreads();
   }
   if (tid == 0) {
-    int sel = 0, executed = 0;
+    int sel = 0, executed = 0, prev = -1;
     for (int d = 0; d < MAX_PASSES; d++) {
       plan->tile_counter[d] = 0;
+      plan->exec_idx[d] = -1;
+      plan->next_shift[d] = -1;
       if (d >= P) {
         plan->src_sel[d] = -1;
         plan->status_sel[d] = 0;
@@ -225,6 +255,9 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
       } else {
         plan->src_sel[d] = sel;
         plan->status_sel[d] = executed & 1;
+        plan->exec_idx[d] = executed;
+        if (prev >= 0) plan->next_shift[prev] = 8 * d;
+        prev = d;
         sel ^= 1;
         executed++;
       }

@@ -112,9 +112,14 @@ struct SlotLayout {
 SlotLayout slot_layout(const hpcs_request& r) {
   SlotLayout l;
   const size_t w = size_t(dtype_bytes(r.dtype));
-  const int64_t units = (r.n + 4095) / 4096;  // the smallest look-back unit of any config
+  const int64_t units = (r.n + 4095) / 4096;  // the smallest tile of any config
   l.keys_bytes = up256(size_t(r.n) * w);
-  l.status_bytes = up256(size_t(units) * 256 * 4);
+  // look-back status words, or the chunked passes' per-range count tables (at most one
+  // range per tile and per SM)
+  const size_t lookback = size_t(units) * 256 * 4;
+  const size_t ranges = size_t(units < 256 ? units : 256);
+  const size_t chunked = ranges * (w + 3) * 256 * 4;
+  l.status_bytes = up256(lookback > chunked ? lookback : chunked);
   size_t o = 0;
   l.a = o;
   o += l.keys_bytes;

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/hpcs_gpu.h"
+#include "chunk_pass.cuh"
 #include "radix_kernels.cuh"
 
 namespace hpcs {
@@ -117,6 +118,47 @@ struct SortConfig<uint64_t, uint32_t, MODE> {
   static constexpr int NT = 512, KPT = 6, STAGES = 2, MINB = 2, CL = HPCS_CL;
 };
 
+// Chunked-pass tile shapes (threads x keys per thread).  Every shape uses two 48 KiB stage
+// buffers, which leaves room for 148 ranges x 512 bytes of next-digit counters within the
+// 227 KiB of shared memory a CTA may use.
+#ifndef HPCS_C32_NT
+#define HPCS_C32_NT 1024
+#endif
+#ifndef HPCS_C32_KPT
+#define HPCS_C32_KPT 12
+#endif
+template <class U, class V, int MODE>
+struct ChunkConfig;
+template <>
+struct ChunkConfig<uint32_t, NoValue, RANK_ORDERED_ATOMIC> {
+  static constexpr int NT = HPCS_C32_NT, KPT = HPCS_C32_KPT;
+};
+template <>
+struct ChunkConfig<uint32_t, NoValue, RANK_PEER_MASK> {  // + lane masks: fewer warps
+  static constexpr int NT = 512, KPT = 20;
+};
+template <int MODE>
+struct ChunkConfig<uint64_t, NoValue, MODE> {
+  static constexpr int NT = 512, KPT = 12;
+};
+template <int MODE>
+struct ChunkConfig<uint32_t, uint32_t, MODE> {
+  static constexpr int NT = 512, KPT = 12;
+};
+template <int MODE>
+struct ChunkConfig<uint64_t, uint32_t, MODE> {
+  static constexpr int NT = 512, KPT = 8;
+};
+constexpr size_t MAX_DYN_SMEM = 232448;  // 227 KiB per CTA on sm_100
+
+template <class U, class V, int MODE>
+struct ChunkShape {
+  using C = ChunkConfig<U, V, MODE>;
+  using L = ChunkSmem<U, V, C::NT, C::KPT, MODE>;
+  static constexpr int TILE = L::TILE;
+  static constexpr int MAX_RANGES = int((MAX_DYN_SMEM - L::BASE_BYTES) / ((RADIX / 2) * 4));
+};
+
 constexpr int HIST_NT = 1024;
 
 // Launches K1 (one CTA per SM, 128 KiB of lane-private counters).
@@ -142,7 +184,8 @@ int launch_histogram(hpcs_ctx* ctx, const U* keys, int64_t n, uint32_t* hist_out
   }
   const int64_t vec = n * int64_t(sizeof(U)) / 16;
   const int64_t want = (vec + HIST_NT * 4 - 1) / (HIST_NT * 4);
-  const int grid = int(want < 1 ? 1 : (want > ctx->sms ? ctx->sms : want));
+  int grid = int(want < 1 ? 1 : (want > ctx->sms ? ctx->sms : want));
+  if (args.chunk_hist) grid = args.chunks;  // CTA j counts key range j
   k<<<grid, HIST_NT, HistSmem<U>::BYTES, s>>>(keys, n, hist_out, args, make_plan);
   HPCS_CUDA(cudaGetLastError());
   return HPCS_OK;
@@ -188,6 +231,45 @@ int launch_onesweep_passes(hpcs_ctx* ctx, SortArgs args, cudaStream_t s) {
   return HPCS_OK;
 }
 
+// Chunked digit passes: one CTA per key range, one launch per digit.
+template <class U, int KIND, class V, int MODE>
+int launch_chunk_passes(hpcs_ctx* ctx, SortArgs args, cudaStream_t s) {
+  using C = ChunkConfig<U, V, MODE>;
+  using L = ChunkSmem<U, V, C::NT, C::KPT, MODE>;
+  constexpr int P = int(sizeof(U));
+  auto k = chunk_pass_kernel<U, KIND, V, C::NT, C::KPT, MODE>;
+  static int attr_set[64] = {0};
+  if (!attr_set[ctx->device & 63]) {
+    HPCS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(MAX_DYN_SMEM)));
+    attr_set[ctx->device & 63] = 1;
+  }
+  const size_t bytes = L::bytes(args.chunks);
+  for (int p = 0; p < P; p++) {
+    args.pass = p;
+    KernelTimer kt(ctx, s, HPCS_K_ONESWEEP);
+    k<<<args.chunks, C::NT, bytes, s>>>(args);
+    HPCS_CUDA(cudaGetLastError());
+  }
+  return HPCS_OK;
+}
+
+// Key ranges of the chunked passes: as many as there are SMs (capped by the counters'
+// shared memory), each a whole number of tiles.
+struct ChunkGeometry {
+  int chunks;
+  uint32_t chunk_keys;
+  uint32_t magic;
+};
+inline ChunkGeometry chunk_geometry(int64_t n, int tile, int max_ranges) {
+  const int64_t tiles = (n + tile - 1) / tile;
+  const int64_t per = (tiles + max_ranges - 1) / max_ranges;  // tiles per range
+  ChunkGeometry g;
+  g.chunks = int((tiles + per - 1) / per);
+  g.chunk_keys = uint32_t(per * tile);
+  g.magic = uint32_t(((uint64_t(1) << 32) + g.chunk_keys - 1) / g.chunk_keys);
+  return g;
+}
+
 // Enqueue a full LSD sort of n keys (and optional 4-byte items) in device memory.
 // keys/vals are sorted in place (with scratch B owned by the context).
 template <class U, int KIND, class V>
@@ -197,9 +279,17 @@ int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t
   constexpr bool PAIRS = !std::is_same<V, NoValue>::value;
   if (n <= 1) return HPCS_OK;
   if (n > MAX_KEYS_PER_SORT) return fail(HPCS_ERR_RANGE, "n exceeds HPCS_MAX_KEYS");
-  const int64_t unit = ctx->rank_mode == RANK_ORDERED_ATOMIC ? int64_t(CA::NT) * CA::KPT * CA::CL
-                                                             : int64_t(CP::NT) * CP::KPT * CP::CL;
-  const int64_t num_tiles = (n + unit - 1) / unit;  // look-back units
+  const bool lookback = ctx->cfg.lookback_passes != 0;
+  const bool ordered = ctx->rank_mode == RANK_ORDERED_ATOMIC;
+  const int64_t unit = ordered ? int64_t(CA::NT) * CA::KPT * CA::CL : int64_t(CP::NT) * CP::KPT * CP::CL;
+  const int64_t num_tiles = lookback ? (n + unit - 1) / unit : 0;  // look-back units
+  ChunkGeometry geo{0, 0, 0};
+  if (!lookback) {
+    using SA = ChunkShape<U, V, RANK_ORDERED_ATOMIC>;
+    using SP = ChunkShape<U, V, RANK_PEER_MASK>;
+    const int cap = ordered ? SA::MAX_RANGES : SP::MAX_RANGES;
+    geo = chunk_geometry(n, ordered ? SA::TILE : SP::TILE, ctx->sms < cap ? ctx->sms : cap);
+  }
 
   // 16-byte alignment is required by the bulk copies; unaligned callers go through A'.
   U* a = keys;
@@ -219,9 +309,10 @@ int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t
     va = static_cast<uint32_t*>(ctx->vals_a.ptr);
     HPCS_CUDA(cudaMemcpyAsync(va, vals, size_t(n) * 4, cudaMemcpyDeviceToDevice, s));
   }
-  const size_t status_bytes = size_t(num_tiles) * RADIX * 4;
+  constexpr int P = int(sizeof(U));
+  const size_t status_bytes = lookback ? size_t(num_tiles) * RADIX * 4 : size_t(geo.chunks) * (P + 3) * RADIX * 4;
   if ((rc = ensure(ctx, ctx->status0, status_bytes)) != HPCS_OK) return rc;
-  if ((rc = ensure(ctx, ctx->status1, status_bytes)) != HPCS_OK) return rc;
+  if (lookback && (rc = ensure(ctx, ctx->status1, status_bytes)) != HPCS_OK) return rc;
   if ((rc = ensure(ctx, ctx->plan, sizeof(SortPlan))) != HPCS_OK) return rc;
 
   SortArgs args{};
@@ -240,6 +331,14 @@ int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t
   args.trace = ctx->trace;
   args.trace_pass = ctx->trace_pass;
   args.trace_capacity = ctx->trace_capacity;
+  if (!lookback) {
+    // status0 holds [chunks][P][256] per-range input counts, then [3][chunks][256] tables
+    args.chunk_hist = static_cast<uint32_t*>(ctx->status0.ptr);
+    args.ctab = args.chunk_hist + size_t(geo.chunks) * P * RADIX;
+    args.chunks = geo.chunks;
+    args.chunk_keys = geo.chunk_keys;
+    args.chunk_magic = geo.magic;
+  }
 
   HPCS_CUDA(cudaMemsetAsync(args.plan, 0, sizeof(SortPlan), s));
 
@@ -248,9 +347,13 @@ int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t
     KernelTimer kt(ctx, s, HPCS_K_HISTOGRAM);
     if ((rc = launch_histogram<U, KIND>(ctx, a, n, &args.plan->hist[0][0], args, 1, s)) != HPCS_OK) return rc;
   }
-  // K3: one onesweep launch per digit
-  rc = ctx->rank_mode == RANK_ORDERED_ATOMIC ? launch_onesweep_passes<U, KIND, V, RANK_ORDERED_ATOMIC>(ctx, args, s)
-                                             : launch_onesweep_passes<U, KIND, V, RANK_PEER_MASK>(ctx, args, s);
+  // K3: one launch per digit
+  if (!lookback)
+    rc = ordered ? launch_chunk_passes<U, KIND, V, RANK_ORDERED_ATOMIC>(ctx, args, s)
+                 : launch_chunk_passes<U, KIND, V, RANK_PEER_MASK>(ctx, args, s);
+  else
+    rc = ordered ? launch_onesweep_passes<U, KIND, V, RANK_ORDERED_ATOMIC>(ctx, args, s)
+                 : launch_onesweep_passes<U, KIND, V, RANK_PEER_MASK>(ctx, args, s);
   if (rc != HPCS_OK) return rc;
   // finalize: result back into the caller's buffer if it ended in B; collect errors
   {

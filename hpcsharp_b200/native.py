@@ -65,7 +65,8 @@ class HpcsConfig(C.Structure):
         ("rank_mode", C.c_int32),
         ("spin_limit_ns", C.c_int64),
         ("poison_tile", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("lookback_passes", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -201,7 +202,8 @@ class Context:
     """One hpcs_ctx: a CUDA stream plus grow-only scratch on one device."""
 
     def __init__(self, device: int = 0, *, pool_bytes: int = 0, skip_trivial_passes: bool = True,
-                 spin_limit_ns: int = 2_000_000_000, poison_tile: int = -1, rank_mode: int = 0):
+                 spin_limit_ns: int = 2_000_000_000, poison_tile: int = -1, rank_mode: int = 0,
+                 lookback_passes: bool = False):
         self.lib = load()
         cfg = default_config()
         cfg.pool_bytes = pool_bytes
@@ -209,6 +211,7 @@ class Context:
         cfg.spin_limit_ns = spin_limit_ns
         cfg.poison_tile = poison_tile
         cfg.rank_mode = rank_mode
+        cfg.lookback_passes = 1 if lookback_passes else 0
         h = C.c_void_p()
         check(self.lib.hpcs_ctx_create(device, C.byref(cfg), C.byref(h)))
         self.handle = h

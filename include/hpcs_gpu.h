@@ -69,8 +69,10 @@ typedef struct hpcs_config {
                                   lane-order probe at context creation (else as 1);
                                   1: always the fully defined peer-mask ranking */
   int64_t spin_limit_ns;       /* bound on every device-side wait (default 2e9) */
-  int32_t poison_tile;         /* test hook: tile that never publishes (-1 = off) */
-  int32_t reserved[7];
+  int32_t poison_tile;         /* test hook: tile whose device wait times out (-1 = off) */
+  int32_t lookback_passes;     /* 0: chunked digit passes (no inter-CTA waiting, default);
+                                  1: single-pass decoupled look-back digit passes */
+  int32_t reserved[6];
 } hpcs_config;
 
 /* ---- context ---------------------------------------------------------------------- */

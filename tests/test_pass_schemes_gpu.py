@@ -1,0 +1,73 @@
+"""The two digit-pass schemes give the oracle's bits: chunked passes (per-range counts
+forwarded from the previous pass, the default) and single-pass decoupled look-back.  Sizes
+put the chunked geometry at its edges: one tile, one range per SM exactly, one tile more
+than there are SMs (ranges of two tiles, half the SMs idle), many tiles per range with a
+short last range, and ragged 16-byte tails."""
+import numpy as np
+import pytest
+
+from hpcsharp_b200 import datagen, native
+
+pytestmark = pytest.mark.gpu
+
+SMS = 148
+TILE = {"u32": 12288, "i32": 12288, "f32": 12288, "u64": 6144, "i64": 6144, "f64": 6144}
+
+
+def _sizes(dt):
+    t = TILE[dt]
+    return [t - 1, t, t + 3, SMS * t, SMS * t + 1, 37 * SMS * t - 5, 5_000_011]
+
+
+@pytest.fixture(scope="module", params=[False, True], ids=["chunked", "lookback"])
+def sctx(request):
+    c = native.Context(0, lookback_passes=request.param)
+    yield c
+    c.close()
+
+
+def _oracle(orc, a):
+    s = a.copy()
+    orc.sort_radix_lsd(s)
+    return s
+
+
+@pytest.mark.parametrize("dt", ["u32", "i32", "f32", "u64", "i64", "f64"])
+def test_scheme_parity_plain(sctx, orc, dt):
+    for n in _sizes(dt):
+        a = datagen.by_name(dt, n, seed=7 + n)
+        got = a.copy()
+        sctx.sort(got)
+        assert np.array_equal(got.view(np.uint8), _oracle(orc, a).view(np.uint8)), (dt, n)
+
+
+@pytest.mark.parametrize("dt", ["u32", "f32", "u64", "f64"])
+def test_scheme_parity_pairs(sctx, orc, dt):
+    for n in (4097, SMS * 6144 + 7, 3_000_017):
+        keys = datagen.by_name(dt, n, seed=11 + n)
+        if dt in ("u32", "u64"):
+            keys = keys % np.array(1000, dtype=keys.dtype)  # heavy duplicates: stability shows
+        items = np.arange(n, dtype=np.uint32)
+        ko, io = keys.copy(), items.copy()
+        orc.sort_pairs(ko, io)
+        kg, ig = keys.copy(), items.copy()
+        sctx.sort_pairs(kg, ig)
+        assert np.array_equal(kg.view(np.uint8), ko.view(np.uint8)), (dt, n)
+        assert np.array_equal(ig, io), (dt, n)
+
+
+@pytest.mark.parametrize("kind", ["constant", "byte1_only", "top_byte_only"])
+def test_scheme_skipped_passes(sctx, orc, kind):
+    """Skipped passes between executed ones: the forwarded counts must be those of the next
+    executed digit."""
+    n = 2_000_003
+    rng = np.random.default_rng(5)
+    if kind == "constant":
+        a = np.full(n, 0xDEADBEEF, dtype=np.uint32)
+    elif kind == "byte1_only":
+        a = (rng.integers(0, 256, n, dtype=np.uint32) << np.uint32(8)) | np.uint32(0x7F0000AA)
+    else:
+        a = (rng.integers(0, 256, n, dtype=np.uint32) << np.uint32(24)) | rng.integers(0, 256, n, dtype=np.uint32)
+    got = a.copy()
+    sctx.sort(got)
+    assert np.array_equal(got, _oracle(orc, a))
