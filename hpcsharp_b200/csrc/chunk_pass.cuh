@@ -143,7 +143,11 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
   if (MODE == RANK_PEER_MASK)
     for (int i = lane; i < 2 * RADIX; i += 32) msk_w[i] = 0u;
 
-  // running start of each digit: bin start + counts of ranges 0..j-1 (G partial sums)
+  // running start of each digit: bin start + counts of ranges 0..j-1 (G partial sums).
+  // The pass before this one does not count this digit's most frequent value h (its
+  // counters would be the most contended); ranges 0..j-1 hold j x L keys, so h's count
+  // is j x L minus the other values' counts.
+  const uint32_t heavy = uint32_t(plan->heavy[pass]);
   {
     const int g = tid / RADIX, d = tid % RADIX;
     uint32_t acc = 0;
@@ -153,10 +157,21 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
   }
   __syncthreads();
   if (tid < RADIX) {
-    uint32_t r = plan->bin_start[pass][tid];
+    uint32_t pre = 0;
 #pragma unroll
-    for (int g = 0; g < G; g++) r += s_cnt[g * RADIX + tid];
-    s_run[tid] = r;
+    for (int g = 0; g < G; g++) pre += s_cnt[g * RADIX + tid];
+    s_run[tid] = plan->bin_start[pass][tid] + pre;
+    uint32_t w = pre;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) w += __shfl_xor_sync(0xFFFFFFFFu, w, o);
+    if (lane == 0) s_wsum[warp] = w;
+  }
+  __syncthreads();
+  if (x > 0 && tid == 0) {
+    uint32_t others = 0;
+#pragma unroll
+    for (int w = 0; w < RADIX / 32; w++) others += s_wsum[w];
+    s_run[heavy] = plan->bin_start[pass][heavy] + uint32_t(j) * LK - others;
   }
   __syncthreads();
 
@@ -164,6 +179,11 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
   const int sd = tid / G, sq = tid % G;  // the digit and warp group this thread scans
   const Digit<U, KIND> dig(shift);
   const Digit<U, KIND> ndig(nshift < 0 ? 0 : nshift);
+  // When the next digit has a frequent value, whole warp instructions of equal keys (runs
+  // of one frequent key after the reorder) would serialise on one counter: such passes
+  // test each instruction for a single (range, value) and add it once.
+  const bool next_skewed = nshift >= 0 && plan->skewed[nshift >> 3] != 0;
+  const uint32_t next_heavy = nshift < 0 ? 0u : uint32_t(plan->heavy[nshift >> 3]);
 
   auto tile_body = [&](auto full_tag, int t) {
     constexpr bool FULL = decltype(full_tag)::value;
@@ -301,8 +321,8 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
         const uint32_t pos = s_gbase[d] + uint32_t(s);
         if (pos < n32) {
           kout_base[pos] = k;
-          if (nshift >= 0) {
-            const uint32_t e = ndig(k);
+          const uint32_t e = ndig(k);
+          if (nshift >= 0 && !next_skewed && e != next_heavy) {
             uint32_t r = __umulhi(pos, magic);
             r -= (r * LK > pos) ? 1u : 0u;
             const uint32_t inc = 1u + (e & 1u) * 0xFFFFu;
@@ -312,6 +332,33 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
           }
         } else {
           out_of_range = true;
+        }
+      }
+    }
+    if (next_skewed) {
+#pragma unroll
+      for (int i = 0; i < KPT; i++) {
+        const int s = i * NT + tid;
+        const U k = key[i];
+        const uint32_t e = ndig(k);
+        const uint32_t pos = s_gbase[dig(k)] + uint32_t(s);
+        uint32_t r = __umulhi(pos, magic);
+        r -= (r * LK > pos) ? 1u : 0u;
+        const bool counted = (FULL || s < tile_n) && pos < n32 && e != next_heavy;
+        const uint32_t word = r * (RADIX / 2) + (e >> 1);
+        const uint32_t unit = 1u + (e & 1u) * 0xFFFFu;
+        const uint32_t code = (word << 1) | (e & 1u);
+        const uint32_t lanes = __ballot_sync(0xFFFFFFFFu, counted);
+        if (lanes == 0u) continue;
+        const int leader = __ffs(lanes) - 1;
+        const uint32_t lead = __shfl_sync(0xFFFFFFFFu, code, leader);
+        const bool one_code = __all_sync(0xFFFFFFFFu, !counted || code == lead);
+        uint32_t inc = counted ? unit : 0u;
+        if (one_code) inc = lane == leader ? unit * uint32_t(__popc(lanes)) : 0u;
+        if (inc) {
+          const uint32_t old = atomicAdd(s_ctab + word, inc);
+          // a half went below 0x8000 to at least 0x8000 (the other half is unchanged)
+          if ((old + inc) & ~old & 0x80008000u) crossed |= 1u << i;
         }
       }
     }

@@ -61,6 +61,8 @@ struct SortPlan {
   uint32_t idle_flag;                     // never written: the wait-timeout test hook spins on it
   int32_t exec_idx[MAX_PASSES];           // 0, 1, 2, ... over the executed passes
   int32_t next_shift[MAX_PASSES];         // bit shift of the next executed pass's digit, -1 if none
+  int32_t heavy[MAX_PASSES];              // the most frequent value of each digit (lowest on ties)
+  int32_t skewed[MAX_PASSES];             // 1 when that value holds more than 1/32 of the keys
 };
 
 struct SortArgs {
@@ -211,14 +213,20 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
   SortPlan* plan = args.plan;
   __shared__ uint32_t s_trivial[P];
   __shared__ uint32_t s_wsum[RADIX / 32];
+  __shared__ unsigned long long s_heavy[P];
   for (int d = 0; d < P; d++) {
     uint32_t c = 0;
     if (tid < RADIX) {
       c = ld_volatile(&hist_out[d * RADIX + tid]);
     }
-    if (tid == 0) s_trivial[d] = 0;
+    if (tid == 0) {
+      s_trivial[d] = 0;
+      s_heavy[d] = 0ull;
+    }
     __syncthreads();
     if (tid < RADIX && int64_t(c) == n) s_trivial[d] = 1;
+    // most frequent value: max of (count, 255 - value)
+    if (tid < RADIX && c) atomicMax(&s_heavy[d], (static_cast<unsigned long long>(c) << 8) | uint32_t(255 - tid));
     // exclusive scan of 256 counts (first 8 warps)
     uint32_t incl = c;
     if (tid < RADIX) {
@@ -243,6 +251,8 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
       plan->tile_counter[d] = 0;
       plan->exec_idx[d] = -1;
       plan->next_shift[d] = -1;
+      plan->heavy[d] = d < P ? int(255u - uint32_t(s_heavy[d] & 255ull)) : 0;
+      plan->skewed[d] = d < P && int64_t(s_heavy[d] >> 8) > n / 32 ? 1 : 0;
       if (d >= P) {
         plan->src_sel[d] = -1;
         plan->status_sel[d] = 0;
@@ -551,7 +561,7 @@ __global__ void __launch_bounds__(NT, MINB) onesweep_pass_kernel(SortArgs args) 
         for (int q = 0; q < CL; q++) {
           const uint32_t v = *cluster_peer(&s_tot[dg], uint32_t(q));
           utot += v;
-          cpre += (uint32_t(q) < crank) ? v : 0u;
+          cpre += (q < int(crank)) ? v : 0u;
         }
       } else {
         utot = s_tot[dg];

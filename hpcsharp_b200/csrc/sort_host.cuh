@@ -118,14 +118,23 @@ struct SortConfig<uint64_t, uint32_t, MODE> {
   static constexpr int NT = 512, KPT = 6, STAGES = 2, MINB = 2, CL = HPCS_CL;
 };
 
-// Chunked-pass tile shapes (threads x keys per thread).  Every shape uses two 48 KiB stage
-// buffers, which leaves room for 148 ranges x 512 bytes of next-digit counters within the
-// 227 KiB of shared memory a CTA may use.
+// Chunked-pass tile shapes (threads x keys per thread).  Every shape keeps its two stage
+// buffers within 128 KiB, which leaves room for 148 ranges x 512 bytes of next-digit
+// counters within the 227 KiB of shared memory a CTA may use.
 #ifndef HPCS_C32_NT
-#define HPCS_C32_NT 1024
+#define HPCS_C32_NT 512
 #endif
 #ifndef HPCS_C32_KPT
-#define HPCS_C32_KPT 12
+#define HPCS_C32_KPT 32
+#endif
+#ifndef HPCS_C64_KPT
+#define HPCS_C64_KPT 16
+#endif
+#ifndef HPCS_CP32_KPT
+#define HPCS_CP32_KPT 16
+#endif
+#ifndef HPCS_CP64_KPT
+#define HPCS_CP64_KPT 10
 #endif
 template <class U, class V, int MODE>
 struct ChunkConfig;
@@ -137,16 +146,29 @@ template <>
 struct ChunkConfig<uint32_t, NoValue, RANK_PEER_MASK> {  // + lane masks: fewer warps
   static constexpr int NT = 512, KPT = 20;
 };
-template <int MODE>
-struct ChunkConfig<uint64_t, NoValue, MODE> {
+template <>
+struct ChunkConfig<uint64_t, NoValue, RANK_ORDERED_ATOMIC> {
+  static constexpr int NT = 512, KPT = HPCS_C64_KPT;
+};
+template <>
+struct ChunkConfig<uint32_t, uint32_t, RANK_ORDERED_ATOMIC> {
+  static constexpr int NT = 512, KPT = HPCS_CP32_KPT;
+};
+template <>
+struct ChunkConfig<uint64_t, uint32_t, RANK_ORDERED_ATOMIC> {
+  static constexpr int NT = 512, KPT = HPCS_CP64_KPT;
+};
+// peer-mask ranking: 32 KiB of lane masks on top, 48 KiB stages
+template <>
+struct ChunkConfig<uint64_t, NoValue, RANK_PEER_MASK> {
   static constexpr int NT = 512, KPT = 12;
 };
-template <int MODE>
-struct ChunkConfig<uint32_t, uint32_t, MODE> {
+template <>
+struct ChunkConfig<uint32_t, uint32_t, RANK_PEER_MASK> {
   static constexpr int NT = 512, KPT = 12;
 };
-template <int MODE>
-struct ChunkConfig<uint64_t, uint32_t, MODE> {
+template <>
+struct ChunkConfig<uint64_t, uint32_t, RANK_PEER_MASK> {
   static constexpr int NT = 512, KPT = 8;
 };
 constexpr size_t MAX_DYN_SMEM = 232448;  // 227 KiB per CTA on sm_100

@@ -11,7 +11,7 @@ from hpcsharp_b200 import datagen, native
 pytestmark = pytest.mark.gpu
 
 SMS = 148
-TILE = {"u32": 12288, "i32": 12288, "f32": 12288, "u64": 6144, "i64": 6144, "f64": 6144}
+TILE = {"u32": 16384, "i32": 16384, "f32": 16384, "u64": 8192, "i64": 8192, "f64": 8192}
 
 
 def _sizes(dt):
@@ -43,7 +43,7 @@ def test_scheme_parity_plain(sctx, orc, dt):
 
 @pytest.mark.parametrize("dt", ["u32", "f32", "u64", "f64"])
 def test_scheme_parity_pairs(sctx, orc, dt):
-    for n in (4097, SMS * 6144 + 7, 3_000_017):
+    for n in (4097, SMS * 8192 + 7, 3_000_017):
         keys = datagen.by_name(dt, n, seed=11 + n)
         if dt in ("u32", "u64"):
             keys = keys % np.array(1000, dtype=keys.dtype)  # heavy duplicates: stability shows
@@ -71,3 +71,28 @@ def test_scheme_skipped_passes(sctx, orc, kind):
     got = a.copy()
     sctx.sort(got)
     assert np.array_equal(got, _oracle(orc, a))
+
+
+@pytest.mark.parametrize("dist", ["zipf", "few_values", "f32_normal"])
+def test_scheme_skewed_digits(sctx, orc, dist):
+    """Digits with frequent values: equal lanes' atomics are grouped (ranks by popcount)
+    and the next pass's most frequent value is derived by subtraction; the bits and the
+    stable order of equal keys still match the oracle."""
+    n = 3_000_017
+    if dist == "zipf":
+        keys = datagen.u64_zipf(n, seed=3)
+    elif dist == "few_values":
+        rng = np.random.default_rng(8)
+        keys = rng.choice(np.array([7, 0xFF00FF, 1 << 40, 3], dtype=np.uint64), size=n, p=[0.6, 0.2, 0.15, 0.05])
+    else:
+        keys = datagen.f32_normal(n, seed=4)
+    got = keys.copy()
+    sctx.sort(got)
+    assert np.array_equal(got.view(np.uint8), _oracle(orc, keys).view(np.uint8))
+    items = np.arange(n, dtype=np.uint32)
+    ko, io = keys.copy(), items.copy()
+    orc.sort_pairs(ko, io)
+    kg, ig = keys.copy(), items.copy()
+    sctx.sort_pairs(kg, ig)
+    assert np.array_equal(kg.view(np.uint8), ko.view(np.uint8))
+    assert np.array_equal(ig, io)
