@@ -147,8 +147,8 @@ def gen_keys(dtype: str, n: int, seed: int = 1) -> np.ndarray:
 
 
 def read_traffic(dtype: str):
-    """DRAM bytes per onesweep launch from the committed ncu summary, if present."""
-    p = os.path.join(ROOT, "profiles", f"onesweep_pass_{dtype}_256M.txt")
+    """DRAM bytes per digit-pass launch from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", f"chunk_pass_{dtype}_256M.txt")
     try:
         for line in open(p):
             if line.startswith("dram_bytes_per_launch="):
@@ -308,13 +308,13 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     value = replicas.weak_scaling_gkeys(n, args.steps, world, total_ms)
     ms_per_step = total_ms / args.steps
 
-    # roofline of the dominant kernel (the onesweep digit pass): algorithmic bytes per
+    # roofline of the dominant kernel (the chunked digit pass): algorithmic bytes per
     # launch = one read + one write of the keys = 2 * n * w
     os_launches, os_ms = prof["onesweep"]
     os_avg_ms = os_ms / max(1, os_launches)
     os_bytes = 2.0 * n * w
     achieved = os_bytes / (os_avg_ms / 1e3) / 1e9 if os_launches else None
-    roof = {"kernel": "onesweep_pass", "bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
+    roof = {"kernel": "chunk_pass", "bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
             "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
             "frac": round(achieved / hbm, 4) if achieved else None,
             "traffic": read_traffic(dtype), "algorithmic_bytes_per_launch": os_bytes,
