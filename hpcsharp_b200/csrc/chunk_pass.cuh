@@ -149,11 +149,23 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
   // is j x L minus the other values' counts.
   const uint32_t heavy = uint32_t(plan->heavy[pass]);
   {
+    // up to 16 independent loads in flight per thread: the sum's latency is a few L2
+    // round trips even for the last range
     const int g = tid / RADIX, d = tid % RADIX;
-    uint32_t acc = 0;
-#pragma unroll 4
-    for (int q = g; q < j; q += G) acc += __ldcg(cin + int64_t(q) * cin_stride + d);
-    s_cnt[g * RADIX + d] = acc;
+    uint32_t acc[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) acc[u] = 0u;
+    for (int q0 = g; q0 < j; q0 += 16 * G) {
+#pragma unroll
+      for (int u = 0; u < 16; u++) {
+        const int q = q0 + u * G;
+        if (q < j) acc[u] += __ldcg(cin + int64_t(q) * cin_stride + d);
+      }
+    }
+    uint32_t sum = 0;
+#pragma unroll
+    for (int u = 0; u < 16; u++) sum += acc[u];
+    s_cnt[g * RADIX + d] = sum;
   }
   __syncthreads();
   if (tid < RADIX) {

@@ -173,6 +173,29 @@ struct ChunkConfig<uint64_t, uint32_t, RANK_PEER_MASK> {
 };
 constexpr size_t MAX_DYN_SMEM = 232448;  // 227 KiB per CTA on sm_100
 
+// Automatic scheme: below these sizes the look-back passes were measured faster on B200 (the
+// chunked passes' per-range count tables cost about J^2 x 256 global adds per pass, which
+// small sorts do not amortise).  u32 keys: equal at 32 Mi, chunked 2% ahead at 64 Mi;
+// u64 keys and u32 pairs: chunked ahead from 8 Mi; u64 + u32 pairs: from 4 Mi.
+template <class U, class V>
+struct ChunkMinKeys;
+template <>
+struct ChunkMinKeys<uint32_t, NoValue> {
+  static constexpr int64_t value = int64_t(48) << 20;
+};
+template <>
+struct ChunkMinKeys<uint64_t, NoValue> {
+  static constexpr int64_t value = int64_t(6) << 20;
+};
+template <>
+struct ChunkMinKeys<uint32_t, uint32_t> {
+  static constexpr int64_t value = int64_t(6) << 20;
+};
+template <>
+struct ChunkMinKeys<uint64_t, uint32_t> {
+  static constexpr int64_t value = int64_t(3) << 20;
+};
+
 template <class U, class V, int MODE>
 struct ChunkShape {
   using C = ChunkConfig<U, V, MODE>;
@@ -301,7 +324,8 @@ int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t
   constexpr bool PAIRS = !std::is_same<V, NoValue>::value;
   if (n <= 1) return HPCS_OK;
   if (n > MAX_KEYS_PER_SORT) return fail(HPCS_ERR_RANGE, "n exceeds HPCS_MAX_KEYS");
-  const bool lookback = ctx->cfg.lookback_passes != 0;
+  const bool lookback = ctx->cfg.pass_scheme == HPCS_PASSES_LOOKBACK ||
+                        (ctx->cfg.pass_scheme != HPCS_PASSES_CHUNKED && n < ChunkMinKeys<U, V>::value);
   const bool ordered = ctx->rank_mode == RANK_ORDERED_ATOMIC;
   const int64_t unit = ordered ? int64_t(CA::NT) * CA::KPT * CA::CL : int64_t(CP::NT) * CP::KPT * CP::CL;
   const int64_t num_tiles = lookback ? (n + unit - 1) / unit : 0;  // look-back units

@@ -65,11 +65,12 @@ class HpcsConfig(C.Structure):
         ("rank_mode", C.c_int32),
         ("spin_limit_ns", C.c_int64),
         ("poison_tile", C.c_int32),
-        ("lookback_passes", C.c_int32),
+        ("pass_scheme", C.c_int32),
         ("reserved", C.c_int32 * 6),
     ]
 
 
+PASS_SCHEMES = {"auto": 0, "lookback": 1, "chunked": 2}
 KCLASS = {"histogram": 0, "onesweep": 1, "finalize": 2, "topk": 3, "segmented": 4}
 
 
@@ -203,7 +204,7 @@ class Context:
 
     def __init__(self, device: int = 0, *, pool_bytes: int = 0, skip_trivial_passes: bool = True,
                  spin_limit_ns: int = 2_000_000_000, poison_tile: int = -1, rank_mode: int = 0,
-                 lookback_passes: bool = False):
+                 pass_scheme: str = "auto"):
         self.lib = load()
         cfg = default_config()
         cfg.pool_bytes = pool_bytes
@@ -211,7 +212,7 @@ class Context:
         cfg.spin_limit_ns = spin_limit_ns
         cfg.poison_tile = poison_tile
         cfg.rank_mode = rank_mode
-        cfg.lookback_passes = 1 if lookback_passes else 0
+        cfg.pass_scheme = PASS_SCHEMES[pass_scheme]
         h = C.c_void_p()
         check(self.lib.hpcs_ctx_create(device, C.byref(cfg), C.byref(h)))
         self.handle = h

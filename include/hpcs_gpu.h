@@ -62,6 +62,9 @@ typedef enum hpcs_dtype {
 
 typedef struct hpcs_ctx hpcs_ctx;
 
+/* Digit-pass schemes (hpcs_config.pass_scheme). */
+enum { HPCS_PASSES_AUTO = 0, HPCS_PASSES_LOOKBACK = 1, HPCS_PASSES_CHUNKED = 2 };
+
 typedef struct hpcs_config {
   int64_t pool_bytes;          /* device scratch budget of the context; 0 = unlimited */
   int32_t skip_trivial_passes; /* 1: skip a digit pass whose keys all share that digit */
@@ -70,8 +73,10 @@ typedef struct hpcs_config {
                                   1: always the fully defined peer-mask ranking */
   int64_t spin_limit_ns;       /* bound on every device-side wait (default 2e9) */
   int32_t poison_tile;         /* test hook: tile whose device wait times out (-1 = off) */
-  int32_t lookback_passes;     /* 0: chunked digit passes (no inter-CTA waiting, default);
-                                  1: single-pass decoupled look-back digit passes */
+  int32_t pass_scheme;         /* digit passes: HPCS_PASSES_AUTO (0, default) picks by key
+                                  type and n; HPCS_PASSES_LOOKBACK (1): single-pass decoupled
+                                  look-back; HPCS_PASSES_CHUNKED (2): per-range counts from
+                                  the previous pass, no inter-CTA waiting */
   int32_t reserved[6];
 } hpcs_config;
 

@@ -1,5 +1,6 @@
 """The two digit-pass schemes give the oracle's bits: chunked passes (per-range counts
-forwarded from the previous pass, the default) and single-pass decoupled look-back.  Sizes
+forwarded from the previous pass) and single-pass decoupled look-back, each forced for every
+size (the automatic choice picks between them by key type and n).  Sizes
 put the chunked geometry at its edges: one tile, one range per SM exactly, one tile more
 than there are SMs (ranges of two tiles, half the SMs idle), many tiles per range with a
 short last range, and ragged 16-byte tails."""
@@ -19,9 +20,9 @@ def _sizes(dt):
     return [t - 1, t, t + 3, SMS * t, SMS * t + 1, 37 * SMS * t - 5, 5_000_011]
 
 
-@pytest.fixture(scope="module", params=[False, True], ids=["chunked", "lookback"])
+@pytest.fixture(scope="module", params=["chunked", "lookback"])
 def sctx(request):
-    c = native.Context(0, lookback_passes=request.param)
+    c = native.Context(0, pass_scheme=request.param)
     yield c
     c.close()
 

@@ -189,14 +189,14 @@ def test_pool_budget_is_enforced(orc):
         c.close()
 
 
-@pytest.mark.parametrize("lookback", [False, True], ids=["chunked", "lookback"])
-def test_device_wait_is_bounded(orc, lookback):
+@pytest.mark.parametrize("scheme", ["chunked", "lookback"])
+def test_device_wait_is_bounded(orc, scheme):
     """Look-back passes: a unit that never publishes (host-set test hook) makes every later
     unit's look-back run out after the spin limit.  Chunked passes: the hooked tile waits on
     a flag that nothing sets.  Either way the call returns HPCS_ERR_DEVICE_TIMEOUT and the
     context stays usable."""
     n = 600_000  # several look-back units after the poisoned one, whatever the unit size
-    c = native.Context(0, spin_limit_ns=20_000_000, poison_tile=1, lookback_passes=lookback)
+    c = native.Context(0, spin_limit_ns=20_000_000, poison_tile=1, pass_scheme=scheme)
     try:
         a = datagen.u32_uniform(n, seed=1)
         with pytest.raises(native.DeviceTimeoutError):
