@@ -381,8 +381,9 @@ def sort_bytes(n: int, w: int) -> int:
 
 
 def run_batched(args, rank: int, world: int, local_rank: int, emit: bool = True):
-    """65,536 arrays of mixed length and dtype: one graph-captured persistent launch vs one
-    plain sort call per array, same arrays, same device."""
+    """65,536 arrays of mixed length and dtype: one graph-captured plan (the arrays binned by
+    length class into the tuned warp- and block-level kernels) vs one plain sort call per array,
+    same arrays, same device."""
     import torch
 
     from hpcsharp_b200 import native, workloads
@@ -410,6 +411,15 @@ def run_batched(args, rank: int, world: int, local_rank: int, emit: bool = True)
             for dt in pools:
                 pools[dt].copy_(pristine[dt])
 
+    tuning = ctx.seg_tuning
+    limits = native.seg_class_limits()
+
+    def cls(n):
+        for c, lim in enumerate(limits):
+            if lim < 0 or n <= lim:
+                return c
+
+    variants_used = sorted({tuning[1 if dt in ("u64", "i64", "f64") else 0][cls(n)] for (_, n), dt in segs})
     plan = ctx.segplan(segs)
     for _ in range(max(1, args.warmup)):
         restore()
@@ -463,7 +473,9 @@ def run_batched(args, rank: int, world: int, local_rank: int, emit: bool = True)
         "roofline": {"bytes": nbytes, "achieved": round(nbytes / (batched_ms / 1e3) / 1e9, 1), "peak": hbm,
                      "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": round(nbytes / (batched_ms / 1e3) / 1e9 / hbm, 4)},
-        "launches": "1 graph (1 persistent kernel) vs " + str(len(segs)) + " plain sort calls",
+        "launches": "1 graph (one persistent launch per kernel variant in use, as concurrent branches) vs "
+                    + str(len(segs)) + " plain sort calls",
+        "seg_tuning": tuning, "variants_used": variants_used,
     }
     if emit and rank == 0:
         line = {"metric": METRIC, "value": out["batched_gkeys_s"], "unit": UNIT, "n_gpus": world,

@@ -26,8 +26,11 @@ NVCC_FLAGS = [
 ]
 
 GPU_SOURCES = ["capi.cu", "noalloc.cu", "segmented_host.cu", "serve.cu"]
-GPU_DEPS = ["common.cuh", "radix_kernels.cuh", "sort_host.cuh", "topk.cuh", "segmented.cuh", "topk_host.cuh",
-            "segmented_host.cuh"]
+
+
+def _gpu_deps() -> list[str]:
+    """Every header of csrc/ (any of them can change the library)."""
+    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh"))
 
 
 def _nvcc() -> str:
@@ -58,7 +61,7 @@ def build_gpu(force: bool = False, verbose_ptxas: bool = False, out: str | None 
     """Compile libhpcs_gpu.so; `defines` (e.g. ["HPCS_K32_KPT=12"]) build a tuning variant."""
     out = out or os.path.join(PKG, "libhpcs_gpu.so")
     srcs = [os.path.join(CSRC, s) for s in GPU_SOURCES]
-    deps = srcs + [os.path.join(CSRC, d) for d in GPU_DEPS] + [os.path.join(ROOT, "include", "hpcs_gpu.h")]
+    deps = srcs + _gpu_deps() + [os.path.join(ROOT, "include", "hpcs_gpu.h")]
     if force or _stale(out, deps):
         flags = list(NVCC_FLAGS)
         if verbose_ptxas:

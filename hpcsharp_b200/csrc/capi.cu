@@ -7,6 +7,7 @@
 
 #include "../../include/hpcs_gpu.h"
 #include "sort_host.cuh"
+#include "segmented_host.cuh"
 #include "topk_host.cuh"
 
 namespace hpcs {
@@ -409,6 +410,7 @@ int hpcs_ctx_create(int device, const hpcs_config* cfg, hpcs_ctx** out) {
     return fail(HPCS_ERR_UNSUPPORTED, "libhpcs_gpu is built for sm_100a (B200)");
   }
   ctx->sms = prop.multiProcessorCount;
+  ctx->seg_tuning = seg_default_tuning();
   if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&ctx->order_event, cudaEventDisableTiming)) != cudaSuccess) {
     delete ctx;
@@ -447,6 +449,12 @@ int hpcs_ctx_destroy(hpcs_ctx* ctx) {
   }
   for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
   if (ctx->order_event) cudaEventDestroy(ctx->order_event);
+  for (int b = 0; b < hpcs_ctx::SEG_BRANCHES; b++) {
+    if (ctx->seg_streams[b]) cudaStreamSynchronize(ctx->seg_streams[b]);
+    if (ctx->seg_streams[b]) cudaStreamDestroy(ctx->seg_streams[b]);
+    if (ctx->seg_join[b]) cudaEventDestroy(ctx->seg_join[b]);
+  }
+  if (ctx->seg_fork) cudaEventDestroy(ctx->seg_fork);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return HPCS_OK;

@@ -250,8 +250,143 @@ __device__ void seg_sort_large(U* keys, U* scratch, int64_t n, unsigned char* sm
   __syncthreads();
 }
 
+// ---- warp-level path: one warp sorts one small segment ----------------------------------
+// Keys stay warp-striped in registers; every pass ranks them with the warp's 2^RB digit
+// counters (RB-bit digits, so 32/RB or 64/RB passes), scans the counters across the lanes
+// and reorders through the warp's own shared buffer.  No CTA barrier is involved, so the
+// warps of a CTA sort different segments independently.
+template <int KPT, int MODE>
+struct WarpSegSmem {
+  static constexpr int BUF_WORDS = 32 * KPT;  // one buffer of u32 words (u64 keys: half as many)
+  static constexpr int CNT_WORDS = RADIX;
+  static constexpr int MSK_WORDS = MODE == RANK_PEER_MASK ? 2 * RADIX : 0;
+  static constexpr int WARP_WORDS = BUF_WORDS + CNT_WORDS + MSK_WORDS;
+  static constexpr int WARPS = 8;  // 256 threads per CTA
+  static constexpr size_t BYTES = size_t(WARPS) * WARP_WORDS * 4;
+};
+
+template <class U, int KIND, int KPTU, int RB, int MODE>
+__device__ void warp_sort_small(U* keys, int n, U* buf, uint32_t* cnt, uint32_t* msk, int lane) {
+  using KO = KeyOrder<U, KIND>;
+  constexpr int RADIX_B = 1 << RB;
+  constexpr int PASSES = (int(sizeof(U)) * 8 + RB - 1) / RB;
+  U key[KPTU];
+  uint32_t rank[KPTU];
+#pragma unroll
+  for (int i = 0; i < KPTU; i++) {
+    const int idx = i * 32 + lane;
+    key[i] = idx < n ? keys[idx] : U(0);
+  }
+  for (int p = 0; p < PASSES; p++) {
+    const int shift = p * RB;
+    for (int i = lane; i < RADIX_B; i += 32) cnt[i] = 0u;
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < KPTU; i++) {
+      const bool valid = i * 32 + lane < n;
+      const uint32_t d = uint32_t(KO::to_ordered(key[i]) >> shift) & uint32_t(RADIX_B - 1);
+      rank[i] = rank_in_warp<MODE>(cnt, msk, d, valid, i & 1, lane);
+    }
+    __syncwarp();
+    // exclusive scan of the counters across the lanes
+    if (RADIX_B >= 32) {
+      constexpr int CPL = RADIX_B >= 32 ? RADIX_B / 32 : 1;
+      uint32_t c[CPL];
+      uint32_t sum = 0;
+#pragma unroll
+      for (int k = 0; k < CPL; k++) {
+        c[k] = cnt[lane * CPL + k];
+        sum += c[k];
+      }
+      uint32_t incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      uint32_t run = incl - sum;
+#pragma unroll
+      for (int k = 0; k < CPL; k++) {
+        cnt[lane * CPL + k] = run;
+        run += c[k];
+      }
+    } else {
+      const uint32_t c = lane < RADIX_B ? cnt[lane] : 0u;
+      uint32_t incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane < RADIX_B) cnt[lane] = incl - c;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < KPTU; i++) {
+      if (i * 32 + lane < n) {
+        const uint32_t d = uint32_t(KO::to_ordered(key[i]) >> shift) & uint32_t(RADIX_B - 1);
+        buf[cnt[d] + rank[i]] = key[i];
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < KPTU; i++) {
+      const int idx = i * 32 + lane;
+      key[i] = idx < n ? buf[idx] : U(0);
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int i = 0; i < KPTU; i++) {
+    const int idx = i * 32 + lane;
+    if (idx < n) keys[idx] = key[i];
+  }
+}
+
+// Persistent warp-level kernel: each warp takes the next segment of its list (all of them at
+// most 32 x KPT u32 / 16 x KPT u64 keys) and sorts it alone.
+template <int KPT, int RB, int MODE>
+__global__ void __launch_bounds__(256) seg_warp_kernel(SegParams prm) {
+  using L = WarpSegSmem<KPT, MODE>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t* base = reinterpret_cast<uint32_t*>(smem) + warp * L::WARP_WORDS;
+  uint32_t* cnt = base + L::BUF_WORDS;
+  uint32_t* msk = cnt + L::CNT_WORDS;
+  if (MODE == RANK_PEER_MASK)
+    for (int i = lane; i < L::MSK_WORDS; i += 32) msk[i] = 0u;
+  __syncwarp();
+  for (;;) {
+    uint32_t sidx = 0;
+    if (lane == 0) sidx = atomicAdd(prm.queue, 1u);
+    sidx = __shfl_sync(0xFFFFFFFFu, sidx, 0);
+    if (int(sidx) >= prm.nsegs) break;
+    const SegDesc sd = prm.segs[sidx];
+    const int n = int(sd.n);
+    if (n <= 1) continue;
+    const bool fits = sd.dtype >= 3 ? n <= 16 * KPT : n <= 32 * KPT;
+    if (!fits) {  // the plan never routes such a segment here
+      if (lane == 0) atomicOr(prm.err, uint32_t(DERR_BOUNDS));
+      continue;
+    }
+    switch (sd.dtype) {
+      case 0: warp_sort_small<uint32_t, KIND_UNSIGNED, KPT, RB, MODE>(static_cast<uint32_t*>(sd.keys), n, base, cnt, msk, lane); break;
+      case 1: warp_sort_small<uint32_t, KIND_SIGNED, KPT, RB, MODE>(static_cast<uint32_t*>(sd.keys), n, base, cnt, msk, lane); break;
+      case 2: warp_sort_small<uint32_t, KIND_FLOAT, KPT, RB, MODE>(static_cast<uint32_t*>(sd.keys), n, base, cnt, msk, lane); break;
+      case 3: warp_sort_small<uint64_t, KIND_UNSIGNED, KPT / 2, RB, MODE>(static_cast<uint64_t*>(sd.keys), n, reinterpret_cast<uint64_t*>(base), cnt, msk, lane); break;
+      case 4: warp_sort_small<uint64_t, KIND_SIGNED, KPT / 2, RB, MODE>(static_cast<uint64_t*>(sd.keys), n, reinterpret_cast<uint64_t*>(base), cnt, msk, lane); break;
+      case 5: warp_sort_small<uint64_t, KIND_FLOAT, KPT / 2, RB, MODE>(static_cast<uint64_t*>(sd.keys), n, reinterpret_cast<uint64_t*>(base), cnt, msk, lane); break;
+      default:
+        if (lane == 0) atomicOr(prm.err, uint32_t(DERR_BOUNDS));
+        break;
+    }
+  }
+}
+
+// ---- block-level path: one CTA sorts one segment (in shared memory when it fits a tile,
+// else tile by tile with running offsets) -------------------------------------------------
 template <int NT, int KPT, int MODE>
-__global__ void __launch_bounds__(NT, 1) segmented_sort_kernel(SegParams prm) {
+__global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) segmented_sort_kernel(SegParams prm) {
   static_assert(NT >= RADIX, "one thread per digit needed");
   using L = SegSmem<NT, KPT, MODE>;
   extern __shared__ __align__(128) unsigned char smem[];

@@ -60,6 +60,13 @@ struct hpcs_ctx {
   // scratch
   hpcs::DevBuf keys_a, keys_b, vals_a, vals_b, status0, status1, plan, counts, err_accum;
   hpcs::DevBuf aux0, aux1, aux2;
+  // batched segmented sort: variant per (key width, length class), and the helper streams
+  // and events that run the launches of different variants concurrently
+  hpcs_seg_tuning seg_tuning{};
+  static constexpr int SEG_BRANCHES = 3;
+  cudaStream_t seg_streams[SEG_BRANCHES] = {};
+  cudaEvent_t seg_fork = nullptr;
+  cudaEvent_t seg_join[SEG_BRANCHES] = {};
 };
 
 namespace hpcs {

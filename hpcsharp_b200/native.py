@@ -78,6 +78,18 @@ class HpcsSegment(C.Structure):
     _fields_ = [("keys", C.c_void_p), ("n", C.c_int64), ("dtype", C.c_int32), ("reserved", C.c_int32)]
 
 
+SEG_CLASSES = 8
+
+
+class HpcsSegTuning(C.Structure):
+    _fields_ = [("variant", (C.c_int32 * SEG_CLASSES) * 2)]
+
+
+class HpcsSegVariantInfo(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("threads", C.c_int32), ("keys_per_thread", C.c_int32),
+                ("digit_bits", C.c_int32), ("max_keys", C.c_int64 * 2)]
+
+
 class HpcsRequest(C.Structure):
     _fields_ = [("op", C.c_int32), ("dtype", C.c_int32), ("input", C.c_void_p), ("output", C.c_void_p),
                 ("n", C.c_int64), ("k", C.c_int64)]
@@ -143,6 +155,11 @@ def _declare(lib) -> None:
     lib.hpcs_segplan_create.argtypes = [P, C.POINTER(HpcsSegment), I64, C.POINTER(P)]
     lib.hpcs_segplan_execute.argtypes = [P, P]
     lib.hpcs_segplan_destroy.argtypes = [P]
+    lib.hpcs_seg_variants.argtypes = [C.POINTER(HpcsSegVariantInfo), I32]
+    lib.hpcs_seg_class_limit.argtypes = [I32]
+    lib.hpcs_seg_class_limit.restype = I64
+    lib.hpcs_ctx_get_seg_tuning.argtypes = [P, C.POINTER(HpcsSegTuning)]
+    lib.hpcs_ctx_set_seg_tuning.argtypes = [P, C.POINTER(HpcsSegTuning)]
     lib.hpcs_server_config_default.argtypes = [C.POINTER(HpcsServerConfig)]
     lib.hpcs_server_config_default.restype = None
     lib.hpcs_server_create.argtypes = [C.POINTER(HpcsServerConfig), C.POINTER(P)]
@@ -176,6 +193,22 @@ def check(status: int) -> None:
     if status == HPCS_ERR_DEVICE_TIMEOUT:
         raise DeviceTimeoutError(status, msg)
     raise HpcsError(status, msg)
+
+
+def seg_variants() -> list[dict]:
+    """The segmented sort's kernel variants (index = variant id)."""
+    lib = load()
+    arr = (HpcsSegVariantInfo * 64)()
+    n = lib.hpcs_seg_variants(arr, 64)
+    return [{"kind": "warp" if arr[i].kind == 0 else "block", "threads": arr[i].threads,
+             "keys_per_thread": arr[i].keys_per_thread, "digit_bits": arr[i].digit_bits,
+             "max_keys": [arr[i].max_keys[0], arr[i].max_keys[1]]} for i in range(n)]
+
+
+def seg_class_limits() -> list[int]:
+    """Upper length limit of each length class of the segmented sort (-1: unbounded)."""
+    lib = load()
+    return [int(lib.hpcs_seg_class_limit(c)) for c in range(SEG_CLASSES)]
 
 
 def default_config() -> HpcsConfig:
@@ -324,6 +357,21 @@ class Context:
 
     def segplan(self, segments) -> "SegPlan":
         return SegPlan(self, segments)
+
+    @property
+    def seg_tuning(self) -> list[list[int]]:
+        """Variant per [4-byte keys, 8-byte keys][length class] of the segmented sort."""
+        t = HpcsSegTuning()
+        check(self.lib.hpcs_ctx_get_seg_tuning(self.handle, C.byref(t)))
+        return [[int(t.variant[w][c]) for c in range(SEG_CLASSES)] for w in range(2)]
+
+    @seg_tuning.setter
+    def seg_tuning(self, table) -> None:
+        t = HpcsSegTuning()
+        for w in range(2):
+            for c in range(SEG_CLASSES):
+                t.variant[w][c] = int(table[w][c])
+        check(self.lib.hpcs_ctx_set_seg_tuning(self.handle, C.byref(t)))
 
     def histogram_dev(self, t, counts, dtype: str | None = None, stream: int | None = None) -> None:
         name = dtype or _torch_dtype_name(t)

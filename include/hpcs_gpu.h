@@ -209,6 +209,35 @@ int hpcs_segplan_create(hpcs_ctx* ctx, const hpcs_segment* segs, int64_t nsegs, 
 int hpcs_segplan_execute(hpcs_segplan* plan, void* stream);
 int hpcs_segplan_destroy(hpcs_segplan* plan);
 
+/* Segmented-sort tuning.  Arrays are classed by length: class c holds the arrays longer than
+ * the limit of class c-1 and at most hpcs_seg_class_limit(c) keys (the last class is
+ * unbounded).  For each key width (index 0: 4-byte keys, 1: 8-byte keys) and class the table
+ * names one kernel variant of hpcs_seg_variants(): a warp-level one (one warp sorts one array
+ * in registers and shared memory) or a block-level one (one CTA per array, in shared memory
+ * when the array fits one tile, else tile by tile with scratch).  A context starts with the
+ * built-in table, chosen on a B200 by the project's autotuner (hpcsharp_b200/autotune.py);
+ * hpcs_ctx_set_seg_tuning replaces it.  A plan uses the table in force when it is created.
+ * Arrays of one variant go to one persistent launch; the launches of different variants run
+ * concurrently on forked streams (inside the plan's graph, as graph branches). */
+#define HPCS_SEG_CLASSES 8
+typedef struct hpcs_seg_tuning {
+  int32_t variant[2][HPCS_SEG_CLASSES];
+} hpcs_seg_tuning;
+typedef struct hpcs_seg_variant_info {
+  int32_t kind;            /* 0: warp level, 1: block level */
+  int32_t threads;         /* threads per CTA */
+  int32_t keys_per_thread; /* 4-byte keys per thread (8-byte keys: half) */
+  int32_t digit_bits;      /* bits per pass */
+  int64_t max_keys[2];     /* longest array it sorts for 4- / 8-byte keys; -1 = any length */
+} hpcs_seg_variant_info;
+/* Fills up to `capacity` entries and returns the number of variants. */
+int hpcs_seg_variants(hpcs_seg_variant_info* out, int capacity);
+/* Upper length limit of class c (-1 for the last, unbounded class; -2 if c is out of range). */
+int64_t hpcs_seg_class_limit(int c);
+int hpcs_ctx_get_seg_tuning(hpcs_ctx* ctx, hpcs_seg_tuning* out);
+/* HPCS_ERR_RANGE if a variant index is unknown or cannot hold the longest array of its class. */
+int hpcs_ctx_set_seg_tuning(hpcs_ctx* ctx, const hpcs_seg_tuning* tuning);
+
 /* ---- radix top-k ---------------------------------------------------------------------
  * Algorithm.SelectTopK(this uint[] a, int k) SelectionTopKRadix.cs:160-171 (and the
  * (a, start, length, k) form :142-153 via a pointer offset): afterwards a[k] is the k-th

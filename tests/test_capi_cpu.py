@@ -64,3 +64,21 @@ def test_ctx_create_reports_missing_device():
     with pytest.raises(native.HpcsError) as e:
         native.Context(0)
     assert e.value.status == native.HPCS_ERR_NO_DEVICE
+
+
+def test_segmented_variants_and_classes_without_gpu():
+    """The segmented sort's variant list and length classes are host-side facts: warp-level
+    variants hold 32 x keys-per-thread 4-byte keys (half for 8-byte keys), block-level ones
+    any length; the classes rise and the last is unbounded."""
+    vs = native.seg_variants()
+    assert len(vs) == 11
+    for v in vs:
+        if v["kind"] == "warp":
+            assert v["max_keys"] == [32 * v["keys_per_thread"], 16 * v["keys_per_thread"]]
+            assert v["digit_bits"] in (4, 8) and v["threads"] == 256
+        else:
+            assert v["max_keys"] == [-1, -1] and v["digit_bits"] == 8
+    limits = native.seg_class_limits()
+    assert limits[-1] == -1 and all(a < b for a, b in zip(limits[:-2], limits[1:-1]))
+    assert native.load().hpcs_seg_class_limit(99) == -2
+    assert native.load().hpcs_ctx_set_seg_tuning(None, None) == native.HPCS_ERR_NULL

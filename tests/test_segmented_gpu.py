@@ -118,3 +118,69 @@ def test_segment_errors(ctx):
     arr[0].dtype = 9
     assert lib.hpcs_sort_segmented_dev(ctx.handle, arr, 1, None) == native.HPCS_ERR_UNSUPPORTED
     assert lib.hpcs_sort_segmented_dev(ctx.handle, None, 0, None) == native.HPCS_OK
+
+
+@pytest.mark.parametrize("variant", list(range(11)))
+def test_every_variant_matches_oracle(orc, variant):
+    """Each kernel variant (warp level with 8- or 4-bit digits, block level with each tile
+    shape), forced onto every length class it can hold, sorts every array of a mixed batch
+    exactly as the oracle sorts it alone, through the one-shot call and a plan."""
+    import torch
+
+    limits = native.seg_class_limits()
+    variants = native.seg_variants()
+    assert len(variants) == 11
+    c = native.Context(0)
+    try:
+        table = c.seg_tuning
+        lengths = []
+        for w in range(2):
+            cap = variants[variant]["max_keys"][w]
+            for cl, lim in enumerate(limits):
+                if cap < 0 or (lim >= 0 and lim <= cap):
+                    table[w][cl] = variant
+        c.seg_tuning = table
+        assert c.seg_tuning == table
+        rng = np.random.default_rng(variant)
+        cap4 = variants[variant]["max_keys"][0]
+        top = cap4 if cap4 > 0 else 40_000
+        lengths = [0, 1, 2, 3, 31, 32, 33, 64, 65] + list((2 ** rng.uniform(1, np.log2(top), size=120)).astype(np.int64))
+        lengths += [top, top - 1]
+        host = make_batch(30 + variant, lengths=lengths)
+        devs = [to_dev(a) if a.size else torch.empty(0, device="cuda") for a, _ in host]
+        segs = [(t, d) for t, (_, d) in zip(devs, host)]
+        c.sort_segmented_dev(segs, stream=torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        c.synchronize()
+        check(host, devs, orc)
+        # the same arrays again through a graph-captured plan
+        for t, (a, _) in zip(devs, host):
+            if a.size:
+                t.copy_(to_dev(a))
+        torch.cuda.synchronize()
+        plan = c.segplan(segs)
+        plan.execute()
+        c.synchronize()
+        check(host, devs, orc)
+        plan.close()
+    finally:
+        c.close()
+
+
+def test_tuning_rejects_a_variant_too_small(ctx):
+    table = ctx.seg_tuning
+    bad = [row[:] for row in table]
+    bad[0][7] = 0  # a 128-key warp variant cannot hold the unbounded class
+    with pytest.raises(native.ArgumentOutOfRangeException):
+        ctx.seg_tuning = bad
+    assert ctx.seg_tuning == table
+
+
+def test_builtin_table_is_the_tuned_record(ctx):
+    import json
+    import os
+
+    from hpcsharp_b200 import autotune
+
+    rec = json.load(open(os.path.join(os.path.dirname(autotune.__file__), "tune", "b200_148sm.json")))
+    assert ctx.seg_tuning == rec["table"]
