@@ -14,12 +14,6 @@
 
 namespace hpcs {
 
-constexpr int SEG_NT = 512, SEG_KPT = 16;  // the serving runtime's coalesced launches
-
-// Keys per tile of the serving runtime's segmented launch for a key width: arrays up to this
-// size are sorted entirely in shared memory and need no scratch.
-inline int64_t seg_tile_keys(int key_bytes) { return int64_t(SEG_NT) * SEG_KPT * 4 / key_bytes; }
-
 // Upper length limits of the length classes (the last is unbounded).
 constexpr int64_t SEG_CLASS_LIMIT[HPCS_SEG_CLASSES] = {128, 256, 512, 2048, 4096, 8192, 65536, -1};
 
@@ -135,18 +129,5 @@ void seg_relocate(std::vector<SegDesc>& table, const std::vector<SegGroup>& grou
 // streams and joined back into `s`.  Zeroes the groups' queues first.
 int seg_launch_groups(hpcs_ctx* ctx, const SegDesc* d_desc, const std::vector<SegGroup>& groups,
                       uint32_t* d_queues, cudaStream_t s);
-
-// The serving runtime's single-variant launch (block level, 512 x 16).
-template <int MODE>
-inline int launch_segmented(hpcs_ctx* ctx, const SegDesc* d_desc, int nsegs, uint32_t* d_queue, cudaStream_t s) {
-  HPCS_CUDA(cudaMemsetAsync(d_queue, 0, 4, s));
-  KernelTimer kt(ctx, s, HPCS_K_SEGMENTED);
-  return launch_seg_variant<MODE>(ctx, 8, d_desc, nsegs, d_queue, s);
-}
-
-inline int enqueue_segmented(hpcs_ctx* ctx, const SegDesc* d_desc, int nsegs, uint32_t* d_queue, cudaStream_t s) {
-  return ctx->rank_mode == RANK_ORDERED_ATOMIC ? launch_segmented<RANK_ORDERED_ATOMIC>(ctx, d_desc, nsegs, d_queue, s)
-                                               : launch_segmented<RANK_PEER_MASK>(ctx, d_desc, nsegs, d_queue, s);
-}
 
 }  // namespace hpcs

@@ -143,11 +143,21 @@ SlotLayout slot_layout(const hpcs_request& r) {
   return l;
 }
 
-// Bytes of a coalesced request: its keys, plus segment scratch if it spans several tiles.
-size_t coalesced_bytes(const hpcs_request& r) {
+// The segmented-sort variant a coalesced request runs with, and whether it needs scratch
+// (a block-level variant whose tile is shorter than the array).
+int coalesced_variant(const hpcs_seg_tuning& t, const hpcs_request& r) {
+  return t.variant[dtype_bytes(r.dtype) == 8 ? 1 : 0][seg_class_of(r.n)];
+}
+bool coalesced_needs_scratch(const hpcs_seg_tuning& t, const hpcs_request& r) {
+  const int v = coalesced_variant(t, r);
+  return SEG_VARIANTS[v].kind == 1 && r.n > seg_variant_tile_keys(v, dtype_bytes(r.dtype));
+}
+
+// Bytes of a coalesced request: its keys, plus segment scratch if its variant needs it.
+size_t coalesced_bytes(const hpcs_seg_tuning& t, const hpcs_request& r) {
   const int w = dtype_bytes(r.dtype);
   size_t b = up256(size_t(r.n) * w);
-  if (r.n > seg_tile_keys(w)) b *= 2;
+  if (coalesced_needs_scratch(t, r)) b *= 2;
   return b;
 }
 
@@ -282,28 +292,40 @@ bool start_on_slot(hpcs_server* sv, hpcs_server::Slot& sl, int slot_idx, Req* q)
   return true;
 }
 
-// Launches the gathered small requests as one segmented sort.
+// Launches the gathered small requests as one segmented sort: the descriptors are ordered by
+// tuned kernel variant (one persistent launch per variant, concurrent) and length.
 void launch_batch(hpcs_server* sv) {
   const size_t n = sv->batch.size();
   hpcs_ctx* c = sv->bctx;
   cudaStream_t s = sv->bstream;
   SegDesc* d_table = reinterpret_cast<SegDesc*>(sv->arena_base + sv->batch_meta_off);
-  uint32_t* d_queue = reinterpret_cast<uint32_t*>(sv->arena_base + sv->batch_meta_off + n * sizeof(SegDesc));
-  for (size_t i = 0; i < n; i++) {
-    Req* q = sv->batch[i];
+  uint32_t* d_queues = reinterpret_cast<uint32_t*>(sv->arena_base + sv->batch_meta_off + n * sizeof(SegDesc));
+  std::vector<size_t> order(n);
+  for (size_t i = 0; i < n; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+    const int va = coalesced_variant(c->seg_tuning, sv->batch[a]->r), vb = coalesced_variant(c->seg_tuning, sv->batch[b]->r);
+    if (va != vb) return va < vb;
+    return sv->batch[a]->r.n * dtype_bytes(sv->batch[a]->r.dtype) > sv->batch[b]->r.n * dtype_bytes(sv->batch[b]->r.dtype);
+  });
+  std::vector<SegGroup> groups;
+  for (size_t j = 0; j < n; j++) {
+    Req* q = sv->batch[order[j]];
     const int w = dtype_bytes(q->r.dtype);
+    const int v = coalesced_variant(c->seg_tuning, q->r);
+    if (groups.empty() || groups.back().variant != v) groups.push_back({v, int(j), 0});
+    groups.back().count++;
     unsigned char* keys = sv->arena_base + q->off;
-    SegDesc& d = sv->host_table[i];
+    SegDesc& d = sv->host_table[j];
     d.keys = keys;
     d.n = q->r.n;
     d.dtype = q->r.dtype;
     d.pad = 0;
-    d.scratch = q->r.n > seg_tile_keys(w) ? keys + up256(size_t(q->r.n) * w) : nullptr;
+    d.scratch = coalesced_needs_scratch(c->seg_tuning, q->r) ? keys + up256(size_t(q->r.n) * w) : nullptr;
     cudaMemcpyAsync(keys, q->r.input, size_t(q->r.n) * w, cudaMemcpyHostToDevice, s);
   }
   cudaMemcpyAsync(d_table, sv->host_table, n * sizeof(SegDesc), cudaMemcpyHostToDevice, s);
   c->last_stream = s;
-  int rc = enqueue_segmented(c, d_table, int(n), d_queue, s);
+  int rc = seg_launch_groups(c, d_table, groups, d_queues, s);
   for (size_t i = 0; i < n; i++) {
     Req* q = sv->batch[i];
     const int w = dtype_bytes(q->r.dtype);
@@ -356,9 +378,9 @@ void scheduler(hpcs_server* sv) {
         if (q->r.n > sv->cfg.coalesce_max_keys) continue;
         if (int(take.size()) >= sv->cfg.coalesce_max_requests) break;
         size_t off = 0;
-        if (!sv->arena.alloc(coalesced_bytes(q->r), &off)) break;
+        if (!sv->arena.alloc(coalesced_bytes(sv->bctx->seg_tuning, q->r), &off)) break;
         q->off = off;
-        q->bytes = coalesced_bytes(q->r);
+        q->bytes = coalesced_bytes(sv->bctx->seg_tuning, q->r);
         q->coalesced = true;
         q->t_admit = now_ns();
         take.push_back(q);
@@ -412,7 +434,7 @@ int check_request(hpcs_server* sv, const hpcs_request* r) {
   if (r->dtype < HPCS_U32 || r->dtype > HPCS_F64) return fail(HPCS_ERR_UNSUPPORTED, "unknown dtype");
   if (r->n <= 0 || r->n > HPCS_MAX_KEYS) return fail(HPCS_ERR_RANGE, "n out of range");
   if (r->op == HPCS_OP_TOPK && (r->k < 0 || r->k > r->n)) return fail(HPCS_ERR_RANGE, "k must be in [0, n]");
-  const size_t need = r->n <= sv->cfg.coalesce_max_keys ? coalesced_bytes(*r) + 256 : slot_layout(*r).total;
+  const size_t need = r->n <= sv->cfg.coalesce_max_keys ? coalesced_bytes(sv->bctx->seg_tuning, *r) + 256 : slot_layout(*r).total;
   if (need > sv->arena.size()) return fail(HPCS_ERR_OOM, "request larger than the server's HBM budget");
   return HPCS_OK;
 }
