@@ -52,9 +52,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps (capped at 20)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served"],
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served", "configs"],
                     help="plain: the 2^28-key sort (headline); batched: 65,536 mixed arrays; "
-                         "served: Poisson sort/top-k requests swept to saturation")
+                         "served: Poisson sort/top-k requests swept to saturation; configs: every "
+                         "plain-sort and pairs configuration, device-resident")
     ap.add_argument("--requests", type=int, default=120, help="served: requests per arrival rate")
     ap.add_argument("--loads", default="0.25,0.5,1,2,4,8,16",
                     help="served: offered loads, as multiples of the plain form's capacity")
@@ -606,6 +607,85 @@ def run_served(args, rank: int, world: int, local_rank: int, emit: bool = True):
     return out
 
 
+def run_configs(args, rank: int, world: int, local_rank: int):
+    """Every plain-sort and key+index configuration, device-resident: the input restored before
+    each of K sorts (outside the CUDA events), Gkeys/s and the fraction of the bytes-moved
+    roofline N*w*(1 + 2P) (+ 2P*N*4 for an index payload)."""
+    import torch
+
+    from hpcsharp_b200 import datagen, native
+
+    if rank != 0:
+        return
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    hbm, peak_kind = peaks()
+    ctx = native.Context(dev)
+    s = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{dev}")
+    steps = max(1, min(args.steps, 10))
+    cfgs = [
+        ("C1 u32 uniform (PCG32 stream)", "u32", 10_000_000, lambda n: datagen.u32_pcg32_stream(n, 1), False),
+        ("C2 u32 uniform", "u32", 1 << 28, lambda n: datagen.u32_uniform(n, 1), False),
+        ("C2 i32 normal(0, 2^20)", "i32", 1 << 28, lambda n: datagen.i32_normal(n, 1), False),
+        ("C2 f32 normal(0,1) + specials", "f32", 1 << 28, lambda n: datagen.f32_normal_special(n, 1), False),
+        ("C2 u64 uniform", "u64", 1 << 27, lambda n: datagen.u64_uniform(n, 1), False),
+        ("C2 u64 AND of 3 uniform", "u64", 1 << 27, lambda n: datagen.u64_and3(n, 1), False),
+        ("C3 u64 Zipf(1.1) keys + u32 index", "u64", 200_000_000, lambda n: datagen.u64_zipf(n, 1), True),
+        ("C3 f64 normal keys + i32 index", "f64", 100_000_000, lambda n: datagen.f64_normal(n, 1), True),
+    ]
+    rows = []
+    for name, dt, n, gen, pairs in cfgs:
+        host = gen(n)
+        w = host.dtype.itemsize
+        P = w
+        tv = torch.int32 if w == 4 else torch.int64
+        pristine = torch.from_numpy(host.view(np.int32 if w == 4 else np.int64)).to(f"cuda:{dev}")
+        buf = pristine.clone()
+        vals = torch.empty(n, dtype=torch.int32, device=f"cuda:{dev}") if pairs else None
+        iota = torch.arange(n, dtype=torch.int32, device=f"cuda:{dev}") if pairs else None
+
+        def restore():
+            with torch.cuda.stream(s):
+                buf.copy_(pristine)
+                if pairs:
+                    vals.copy_(iota)
+
+        def sort():
+            if pairs:
+                ctx.sort_pairs_dev(buf, vals, dtype=dt, stream=ctx.stream)
+            else:
+                ctx.sort_dev(buf, dtype=dt, stream=ctx.stream)
+
+        for _ in range(max(3, args.warmup)):
+            restore()
+            sort()
+        ctx.synchronize()
+        tot = 0.0
+        for _ in range(steps):
+            restore()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            sort()
+            b.record(s)
+            ctx.synchronize()
+            tot += a.elapsed_time(b)
+        ms = tot / steps
+        nbytes = n * w * (1 + 2 * P) + (2 * P * n * 4 if pairs else 0)
+        achieved = nbytes / (ms / 1e3) / 1e9
+        o = buf[:1 << 20].cpu().numpy().view(host.dtype)
+        if not _in_order(o):
+            raise RuntimeError(f"{name}: result not in order")
+        rows.append({"config": name, "dtype": dt, "n": n, "pairs": pairs, "ms": round(ms, 3),
+                     "gkeys_s": round(n / (ms / 1e3) / 1e9, 3), "algorithmic_bytes": nbytes,
+                     "achieved_gbs": round(achieved, 1), "roofline_frac": round(achieved / hbm, 4),
+                     "l2": "inputs larger than L2" if n * w > (126 << 20) else "input fits in L2 (not graded)"})
+        del pristine, buf, vals, iota
+        torch.cuda.empty_cache()
+    ctx.close()
+    print(json.dumps({"metric": METRIC, "workload": "configs", "unit": UNIT, "peak": hbm, "peak_kind": peak_kind,
+                      "steps": steps, "rows": rows}), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -619,6 +699,9 @@ def main():
         return
     if args.workload == "served":
         run_served(args, rank, world, local_rank)
+        return
+    if args.workload == "configs":
+        run_configs(args, rank, world, local_rank)
         return
     run_ours(args, rank, world, local_rank)
 
