@@ -9,9 +9,13 @@ Reference surface (paths relative to the HPCsharp project root):
   Algorithm.SortRadixLsdFunc(this T[] [, int start, int length])       RadixSortLsd.cs:238, :315, :400, :490
   Algorithm.SortRadix(this uint[]) (examples' spelling, Program.cs:26)
   Algorithm.SortRadix<T>(this T[] items, UInt32[]/UInt64[] keys)        RadixSortLsd.cs:1183, :1245
+  Algorithm.SortRadixLsd<T>(this T[], Func<T, UInt32/UInt64> getKey)    RadixSortLsd.cs:714, :783
+  Algorithm.SortRadixFaster<T>(this T[], Func<T, UInt32/UInt64> getKey) RadixSortLsd.cs:861, :961
   Algorithm.HistogramByteComponents(T[], int l, int r)                 Histogram.cs:261, :957, :992, :1019
   ParallelAlgorithm.HistogramByteComponentsPar(T[], int l, int r, ...)  HistogramParallel.cs:214, :416, :547, :617
   Algorithm.SelectTopK(this uint[], int k) / (a, start, length, k)     SelectionTopKRadix.cs:160, :142
+  Algorithm.SelectRadix(this uint[]/ulong[], k or int[] k [, start, length])
+                                                                       SelectionRadix.cs:236-435
 
 Arrays are numpy arrays sorted in place (the reference's SortRadixPar returns the caller's
 array after an even number of passes, RadixSortLsdParallel.cs:227-231).  float32/float64
@@ -42,11 +46,17 @@ def SortRadixInPlaceInterfacePar(inputArray: np.ndarray) -> None:
     default_context().sort(inputArray)
 
 
-def SortRadixLsd(inOutArray: np.ndarray, startIndex: int | None = None, length: int | None = None) -> None:
+def SortRadixLsd(inOutArray, startIndex=None, length: int | None = None):
     """In-place serial-API sort; with (startIndex, length) sorts that subrange in place.
     (The reference's subrange overload writes its result to [0, length) because
     ComputeStartOfBins starts every bin at 0, RadixSortLsd.cs:120; this sorts the
-    subrange where it lies.)"""
+    subrange where it lies.)
+
+    SortRadixLsd(items, getKey) is the user-defined-type form (RadixSortLsd.cs:714, :783):
+    returns a new list of the items in stable ascending order of getKey(item), an unsigned
+    32- or 64-bit key (64-bit when any key exceeds 2^32 - 1)."""
+    if callable(startIndex):
+        return _sort_by_key(inOutArray, startIndex)
     _require(inOutArray, "inOutArray")
     if startIndex is None:
         default_context().sort(inOutArray)
@@ -54,6 +64,27 @@ def SortRadixLsd(inOutArray: np.ndarray, startIndex: int | None = None, length: 
     if length is None or startIndex < 0 or length < 0 or startIndex + length > inOutArray.size:
         raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "startIndex/length outside the array")
     default_context().sort(inOutArray[startIndex:startIndex + length])
+
+
+def _sort_by_key(inputArray, getKey):
+    """Keys extracted on the host, sorted on the GPU with their indices as the payload, items
+    gathered by the sorted indices."""
+    _require(inputArray, "inputArray")
+    _require(getKey, "getKey")
+    items = list(inputArray)
+    keys = np.fromiter((int(getKey(x)) for x in items), dtype=np.uint64, count=len(items))
+    if keys.size and int(keys.max()) <= 0xFFFFFFFF:
+        keys = keys.astype(np.uint32)
+    index = np.arange(len(items), dtype=np.uint32)
+    if len(items):
+        default_context().sort_pairs(keys, index)
+    return [items[i] for i in index]
+
+
+def SortRadixFaster(inputArray, getKey):
+    """SortRadixFaster<T>(this T[], Func<T, UInt32/UInt64>) RadixSortLsd.cs:861, :961: the
+    same stable key-order result as SortRadixLsd(items, getKey)."""
+    return _sort_by_key(inputArray, getKey)
 
 
 def SortRadixLsdFunc(inOutArray: np.ndarray, startIndex: int | None = None, length: int | None = None):
@@ -110,3 +141,37 @@ def SelectTopK(arrayToBeSelected: np.ndarray, *args) -> None:
     if k < start or k >= start + length:
         raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "k must be between start and (start + length)")
     default_context().select_topk(a[start:start + length], k - start)
+
+
+def SelectRadix(arrayToBeSelected: np.ndarray, *args):
+    """SelectRadix (SelectionRadix.cs:236-435), in place, on the GPU's radix select:
+      SelectRadix(a, k) / SelectRadix(a, start, length, k) -> the k-th smallest key (0-based;
+        k indexes the whole array), left at a[k] with a[k..] holding the larger keys;
+      SelectRadix(a, k_list) / SelectRadix(a, start, length, k_list) -> None; afterwards every
+        a[k_i] holds the k_i-th smallest key of the (sub)array.  The several-k form sorts the
+        (sub)array, which satisfies every k at once."""
+    _require(arrayToBeSelected, "arrayToBeSelected")
+    a = arrayToBeSelected
+    if len(args) in (1, 3) and np.ndim(args[-1]) == 1:
+        ks = [int(x) for x in args[-1]]
+        start, length = (0, a.size) if len(args) == 1 else (int(args[0]), int(args[1]))
+        if start < 0 or length <= 0 or start + length > a.size:
+            raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "l or r are invalid")
+        for k in ks:
+            if k < start or k >= start + length:
+                raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "k must be between start and (start + length)")
+        default_context().sort(a[start:start + length])
+        return None
+    if len(args) == 1:
+        k = int(args[0])
+        if a.size <= 0 or k < 0 or k >= a.size:
+            raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "k must be between start and (start + length)")
+        default_context().select_topk(a, k)
+        return a[k]
+    start, length, k = (int(x) for x in args)
+    if start < 0 or length <= 0 or start + length > a.size:
+        raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "l or r are invalid")
+    if k < start or k >= start + length:
+        raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "k must be between start and (start + length)")
+    default_context().select_topk(a[start:start + length], k - start)
+    return a[k]

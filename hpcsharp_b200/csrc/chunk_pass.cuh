@@ -195,6 +195,13 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
   // of one frequent key after the reorder) would serialise on one counter: such passes
   // test each instruction for a single (range, value) and add it once.
   const bool next_skewed = nshift >= 0 && plan->skewed[nshift >> 3] != 0;
+  // When this pass's two most frequent values hold more than 3/4 of the keys (e.g. the top
+  // byte of small signed values: 0x7F and 0x80), their lanes rank with one atomic per warp
+  // instruction each (ordered-atomic mode only).  Measured on B200: +10% for normal(0, 2^20)
+  // int32 keys; below 3/4 (floats' top byte, sparse-bit keys) the votes cost more than the
+  // serialised atomics they replace.
+  const bool grouped = MODE == RANK_ORDERED_ATOMIC && plan->grouped[pass] != 0;
+  const uint32_t heavy2 = uint32_t(plan->heavy2[pass]);
   const uint32_t next_heavy = nshift < 0 ? 0u : uint32_t(plan->heavy[nshift >> 3]);
 
   auto tile_body = [&](auto full_tag, int t) {
@@ -242,10 +249,18 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
       else if (idx < tile_n) k = kin[tile_base + idx];
       key[i] = k;
     }
+    if (grouped) {
 #pragma unroll
-    for (int i = 0; i < KPT; i++) {
-      const int idx = wbase + i * 32 + lane;
-      rank[i] = rank_in_warp<MODE>(cnt_w, msk_w, dig(key[i]), FULL || idx < tile_n, i & 1, lane);
+      for (int i = 0; i < KPT; i++) {
+        const int idx = wbase + i * 32 + lane;
+        rank[i] = rank_in_warp_top2(cnt_w, dig(key[i]), FULL || idx < tile_n, heavy, heavy2, lane);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < KPT; i++) {
+        const int idx = wbase + i * 32 + lane;
+        rank[i] = rank_in_warp<MODE>(cnt_w, msk_w, dig(key[i]), FULL || idx < tile_n, i & 1, lane);
+      }
     }
     __syncthreads();  // (A) warp counts complete; the stage buffer is no longer read
     if (trace) trace[4] = global_timer_ns();

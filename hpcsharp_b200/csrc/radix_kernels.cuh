@@ -63,6 +63,8 @@ struct SortPlan {
   int32_t next_shift[MAX_PASSES];         // bit shift of the next executed pass's digit, -1 if none
   int32_t heavy[MAX_PASSES];              // the most frequent value of each digit (lowest on ties)
   int32_t skewed[MAX_PASSES];             // 1 when that value holds more than 1/32 of the keys
+  int32_t heavy2[MAX_PASSES];             // the second most frequent value
+  int32_t grouped[MAX_PASSES];            // 1 when the two hold more than 3/4 of the keys
 };
 
 struct SortArgs {
@@ -214,6 +216,7 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
   __shared__ uint32_t s_trivial[P];
   __shared__ uint32_t s_wsum[RADIX / 32];
   __shared__ unsigned long long s_heavy[P];
+  __shared__ unsigned long long s_heavy2[P];
   for (int d = 0; d < P; d++) {
     uint32_t c = 0;
     if (tid < RADIX) {
@@ -222,11 +225,15 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
     if (tid == 0) {
       s_trivial[d] = 0;
       s_heavy[d] = 0ull;
+      s_heavy2[d] = 0ull;
     }
     __syncthreads();
     if (tid < RADIX && int64_t(c) == n) s_trivial[d] = 1;
-    // most frequent value: max of (count, 255 - value)
-    if (tid < RADIX && c) atomicMax(&s_heavy[d], (static_cast<unsigned long long>(c) << 8) | uint32_t(255 - tid));
+    // most frequent value: max of (count, 255 - value); then the most frequent of the others
+    const unsigned long long packed = (static_cast<unsigned long long>(c) << 8) | uint32_t(255 - tid);
+    if (tid < RADIX && c) atomicMax(&s_heavy[d], packed);
+    __syncthreads();
+    if (tid < RADIX && c && packed != s_heavy[d]) atomicMax(&s_heavy2[d], packed);
     // exclusive scan of 256 counts (first 8 warps)
     uint32_t incl = c;
     if (tid < RADIX) {
@@ -253,6 +260,8 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
       plan->next_shift[d] = -1;
       plan->heavy[d] = d < P ? int(255u - uint32_t(s_heavy[d] & 255ull)) : 0;
       plan->skewed[d] = d < P && int64_t(s_heavy[d] >> 8) > n / 32 ? 1 : 0;
+      plan->heavy2[d] = d < P && s_heavy2[d] ? int(255u - uint32_t(s_heavy2[d] & 255ull)) : plan->heavy[d];
+      plan->grouped[d] = d < P && int64_t(s_heavy[d] >> 8) + int64_t(s_heavy2[d] >> 8) > n / 4 * 3 ? 1 : 0;
       if (d >= P) {
         plan->src_sel[d] = -1;
         plan->status_sel[d] = 0;
@@ -317,6 +326,30 @@ __device__ __forceinline__ uint32_t rank_in_warp(uint32_t* cnt, uint32_t* msk, u
     }
     return before + __popc(lt);
   }
+}
+
+// Ordered-atomic ranking for a pass whose two most frequent digit values h1, h2 hold much of
+// the keys: the lanes of a warp instruction holding h1 (or h2) take one atomicAdd of their
+// count, made by the lowest of them, and rank among themselves by popcount, instead of
+// serialising on one counter; other lanes rank with their own atomic.  Same ranks as
+// rank_in_warp<RANK_ORDERED_ATOMIC>.  All lanes must call it (it uses warp votes).
+__device__ __forceinline__ uint32_t rank_in_warp_top2(uint32_t* cnt, uint32_t d, bool valid, uint32_t h1,
+                                                      uint32_t h2, int lane) {
+  const bool is1 = valid && d == h1;
+  const bool is2 = valid && d == h2 && h2 != h1;
+  const uint32_t m1 = __ballot_sync(0xFFFFFFFFu, is1);
+  const uint32_t m2 = __ballot_sync(0xFFFFFFFFu, is2);
+  const int l1 = m1 ? __ffs(m1) - 1 : 0;
+  const int l2 = m2 ? __ffs(m2) - 1 : 0;
+  uint32_t b1 = 0, b2 = 0, r = 0;
+  if (m1 && lane == l1) b1 = atomicAdd(&cnt[h1], uint32_t(__popc(m1)));
+  if (m2 && lane == l2) b2 = atomicAdd(&cnt[h2], uint32_t(__popc(m2)));
+  if (valid && !is1 && !is2) r = atomicAdd(&cnt[d], 1u);
+  b1 = __shfl_sync(0xFFFFFFFFu, b1, l1);
+  b2 = __shfl_sync(0xFFFFFFFFu, b2, l2);
+  if (is1) r = b1 + uint32_t(__popc(m1 & lanemask_lt()));
+  if (is2) r = b2 + uint32_t(__popc(m2 & lanemask_lt()));
+  return r;
 }
 
 template <class U, class V, int NT, int KPT, int STAGES, int MODE>

@@ -16,6 +16,7 @@
 #include <stdexcept>
 #include <string>
 #include <utility>
+#include <type_traits>
 #include <vector>
 
 #include "hpcs_gpu.h"
@@ -198,6 +199,32 @@ struct Algorithm {
   static std::vector<std::vector<uint32_t>> HistogramByteComponents(const std::vector<T>& inArray, int64_t l,
                                                                     int64_t r) {
     return ParallelAlgorithm::HistogramByteComponentsPar(inArray, l, r);
+  }
+  // SortRadixLsd<T>(this T[] inputArray, Func<T, UInt32/UInt64> getKey) RadixSortLsd.cs:714,
+  // :783 (and SortRadixFaster<T>, :861, :961): a new array of the elements in stable
+  // ascending order of getKey.  The keys are extracted on the host, sorted on the GPU with
+  // their indices as the payload, and the elements gathered by the sorted indices.
+  template <class T, class F>
+  static std::vector<T> SortRadixLsd(const std::vector<T>& inputArray, F getKey) {
+    using K = typename std::decay<decltype(getKey(inputArray[0]))>::type;
+    static_assert(std::is_same<K, uint32_t>::value || std::is_same<K, uint64_t>::value,
+                  "getKey returns UInt32 or UInt64");
+    const size_t n = inputArray.size();
+    std::vector<K> keys(n);
+    std::vector<uint32_t> index(n);
+    for (size_t i = 0; i < n; i++) {
+      keys[i] = getKey(inputArray[i]);
+      index[i] = uint32_t(i);
+    }
+    SortRadix(index, keys);
+    std::vector<T> out;
+    out.reserve(n);
+    for (size_t i = 0; i < n; i++) out.push_back(inputArray[index[i]]);
+    return out;
+  }
+  template <class T, class F>
+  static std::vector<T> SortRadixFaster(const std::vector<T>& inputArray, F getKey) {
+    return SortRadixLsd(inputArray, getKey);
   }
 };
 

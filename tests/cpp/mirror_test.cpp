@@ -69,6 +69,24 @@ int main() {
   for (int64_t i = 10; i <= 99989; i++) want[h[i] & 0xFF]++;
   CHECK(counts.size() == 4 && counts[0] == want);
 
+  // SortRadixLsd<T>(items, getKey): stable by the extracted key, new array
+  struct Rec {
+    uint32_t id;
+    uint64_t score;
+  };
+  std::vector<Rec> recs(50000);
+  for (size_t i = 0; i < recs.size(); i++) recs[i] = {uint32_t(i), uint64_t(rng() % 1000) << 40 | (rng() % 7)};
+  auto by32 = Algorithm::SortRadixLsd(recs, [](const Rec& r) { return uint32_t(r.score >> 40); });
+  auto by64 = Algorithm::SortRadixFaster(recs, [](const Rec& r) { return r.score; });
+  std::vector<Rec> w32 = recs, w64 = recs;
+  std::stable_sort(w32.begin(), w32.end(), [](const Rec& a, const Rec& b) { return (a.score >> 40) < (b.score >> 40); });
+  std::stable_sort(w64.begin(), w64.end(), [](const Rec& a, const Rec& b) { return a.score < b.score; });
+  bool same32 = by32.size() == w32.size(), same64 = by64.size() == w64.size();
+  for (size_t i = 0; same32 && i < w32.size(); i++) same32 = by32[i].id == w32[i].id;
+  for (size_t i = 0; same64 && i < w64.size(); i++) same64 = by64[i].id == w64[i].id;
+  CHECK(same32);
+  CHECK(same64);
+
   // exceptions mirror the reference's
   bool threw = false;
   try {

@@ -237,3 +237,17 @@ def test_peer_mask_ranking_parity(orc, dt):
         assert_same_bits(got, want)
     finally:
         c.close()
+
+
+@pytest.mark.parametrize("wide", [False, True])
+def test_user_defined_type_sort_by_key(wide):
+    """SortRadixLsd(items, getKey) / SortRadixFaster: stable ascending by the extracted key, a
+    new list, equal to Python's stable sort by the same key."""
+    rng = np.random.default_rng(9)
+    n = 200_003
+    hi = (1 << 40) if wide else 1000
+    items = [(int(k), i) for i, k in enumerate(rng.integers(0, hi, size=n, dtype=np.uint64))]
+    want = sorted(items, key=lambda t: t[0])
+    assert algorithm.SortRadixLsd(items, lambda t: t[0]) == want
+    assert algorithm.SortRadixFaster(items, lambda t: t[0]) == want
+    assert algorithm.SortRadixLsd([], lambda t: t) == []

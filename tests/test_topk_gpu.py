@@ -134,3 +134,30 @@ def test_topk_golden(ctx):
     assert int(b[g["k"]]) == g["kth_value"]
     top = np.sort(b[g["k"]:])
     assert hashlib.sha256(top.view(np.uint8).tobytes()).hexdigest() == g["top_sorted_sha256"]
+
+
+@pytest.mark.parametrize("dt", ["u32", "u64", "i32", "f32"])
+def test_select_radix_contract(dt):
+    """SelectRadix(a, k) returns the k-th smallest key and leaves it at a[k] (larger keys
+    after it); SelectRadix(a, start, length, k) does so within the subarray with k indexing
+    the whole array; SelectRadix(a, [k...]) leaves every a[k_i] at the k_i-th smallest."""
+    a0 = datagen.by_name(dt, 300_007, seed=77)
+    srt = a0.copy()
+    native.default_context().sort(srt)
+    for k in (0, 1, 150_000, 300_006):
+        a = a0.copy()
+        v = algorithm.SelectRadix(a, k)
+        assert v.tobytes() == srt[k].tobytes() and a[k].tobytes() == srt[k].tobytes()
+    a = a0.copy()
+    v = algorithm.SelectRadix(a, 1000, 50_000, 20_000)
+    sub = a0[1000:51_000].copy()
+    native.default_context().sort(sub)
+    assert v.tobytes() == sub[19_000].tobytes()
+    assert np.array_equal(a[:1000], a0[:1000]) and np.array_equal(a[51_000:], a0[51_000:])
+    a = a0.copy()
+    ks = np.array([3, 99, 12_345, 299_000])
+    assert algorithm.SelectRadix(a, ks) is None
+    for k in ks:
+        assert a[k].tobytes() == srt[k].tobytes()
+    with pytest.raises(native.ArgumentOutOfRangeException):
+        algorithm.SelectRadix(a0.copy(), a0.size)
