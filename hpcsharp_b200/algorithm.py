@@ -14,6 +14,7 @@ Reference surface (paths relative to the HPCsharp project root):
   Algorithm.HistogramByteComponents(T[], int l, int r)                 Histogram.cs:261, :957, :992, :1019
   ParallelAlgorithm.HistogramByteComponentsPar(T[], int l, int r, ...)  HistogramParallel.cs:214, :416, :547, :617
   Algorithm.SelectTopK(this uint[], int k) / (a, start, length, k)     SelectionTopKRadix.cs:160, :142
+  Algorithm.SortRadixMsd(this float[]/double[]/...)                       RadixSortMsd.cs:1563-1610
   Algorithm.SelectRadix(this uint[]/ulong[], k or int[] k [, start, length])
                                                                        SelectionRadix.cs:236-435
 
@@ -175,3 +176,11 @@ def SelectRadix(arrayToBeSelected: np.ndarray, *args):
         raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "k must be between start and (start + length)")
     default_context().select_topk(a[start:start + length], k - start)
     return a[k]
+
+
+def SortRadixMsd(arrayToBeSorted: np.ndarray) -> np.ndarray:
+    """SortRadixMsd(this float[]/double[]) RadixSortMsd.cs:1563-1610 (and the integer forms):
+    ascending order under the same float/signed transforms, in place.  The LSD sort gives the
+    identical result (equal keys are identical bit patterns, so stability is unobservable)."""
+    _require(arrayToBeSorted, "arrayToBeSorted")
+    return default_context().sort(arrayToBeSorted)

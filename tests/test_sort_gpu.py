@@ -251,3 +251,11 @@ def test_user_defined_type_sort_by_key(wide):
     assert algorithm.SortRadixLsd(items, lambda t: t[0]) == want
     assert algorithm.SortRadixFaster(items, lambda t: t[0]) == want
     assert algorithm.SortRadixLsd([], lambda t: t) == []
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64", "i32"])
+def test_sort_radix_msd_alias(ctx, orc, dt):
+    a = datagen.by_name(dt, 100_003, seed=5)
+    want = oracle_sorted(orc, a)
+    got = algorithm.SortRadixMsd(a.copy())
+    assert_same_bits(got, want)
