@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--requests", type=int, default=120, help="served: requests per arrival rate")
     ap.add_argument("--loads", default="0.25,0.5,1,2,4,8,16",
                     help="served: offered loads, as multiples of the plain form's capacity")
+    ap.add_argument("--arrays", type=int, default=65536,
+                    help="batched: number of arrays (the scaled total keeps ~3,815 keys per array)")
     ap.add_argument("--literal", action="store_true",
                     help="batched: the literal length distribution (~6.6 G keys) instead of ~250 M")
     return ap.parse_args()
@@ -391,8 +393,8 @@ def run_batched(args, rank: int, world: int, local_rank: int, emit: bool = True)
 
     dev = local_rank
     torch.cuda.set_device(dev)
-    lengths, dtypes = workloads.batched_lengths(target_total=None if args.literal else 250_000_000,
-                                                seed=4 + rank)
+    lengths, dtypes = workloads.batched_lengths(
+        count=args.arrays, target_total=None if args.literal else 250_000_000 * args.arrays // 65536, seed=4 + rank)
     bset = workloads.BatchedSet(lengths, dtypes, seed=1 + rank)
     tv = {4: (torch.int32, np.int32), 8: (torch.int64, np.int64)}
     pools, pristine = {}, {}
