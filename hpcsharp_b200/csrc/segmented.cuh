@@ -15,6 +15,7 @@
 // lane-order probe, or the peer-mask ranking).
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 #include "common.cuh"
 #include "radix_kernels.cuh"
@@ -35,6 +36,7 @@ struct SegParams {
   int nsegs;
   uint32_t* queue;  // next segment index (zeroed before each launch)
   uint32_t* err;    // device error bits
+  uint64_t spin_limit_ns;  // bound on the bulk-copy waits
 };
 
 template <int NT, int KPT, int MODE>
@@ -51,7 +53,8 @@ struct SegSmem {
   static constexpr size_t OFF_GBASE = OFF_LOCAL + RADIX * 4;
   static constexpr size_t OFF_WSUM = OFF_GBASE + RADIX * 4;
   static constexpr size_t OFF_SEG = OFF_WSUM + 32 * 4;
-  static constexpr size_t BYTES = OFF_SEG + 16;
+  static constexpr size_t OFF_MBAR = (OFF_SEG + 16 + 7) / 8 * 8;  // [2] bulk-copy barriers
+  static constexpr size_t BYTES = OFF_MBAR + 16;
 };
 
 // Ranks one tile of keys held warp-striped in registers (key i of lane l = tile position
@@ -157,13 +160,19 @@ __device__ void seg_sort_small(U* keys, int n, unsigned char* smem) {
 
 // A segment larger than one tile: histogram every digit in one read, then per pass the
 // tiles in order with running per-digit offsets (ping-pong with the segment's scratch).
+// When the segment spans at least 8 tiles and its keys are 16-byte aligned, each tile is
+// staged by a 1-D bulk async copy into one of the two tile buffers, issued two tiles ahead,
+// so the next tile's load overlaps this tile's ranking and scatter; the ragged tail under 16
+// bytes is read with plain loads.  (Shorter segments were measured faster with plain loads:
+// the copies' barriers and proxy fences cost more than the latency they hide.)
+// `phase` carries the two mbarriers' expected parities across the segments a CTA sorts.
 template <class U, int KIND, int NT, int KPT, int MODE>
-__device__ void seg_sort_large(U* keys, U* scratch, int64_t n, unsigned char* smem, uint32_t* err) {
+__device__ void seg_sort_large(U* keys, U* scratch, int64_t n, unsigned char* smem, uint32_t* err,
+                               uint64_t spin_limit_ns, uint32_t& phase) {
   using KO = KeyOrder<U, KIND>;
   using L = SegSmem<NT, KPT * int(sizeof(U)) / 4, MODE>;
   constexpr int P = int(sizeof(U));
   constexpr int TILE = NT * KPT;
-  U* sk = reinterpret_cast<U*>(smem + L::OFF_BUF);
   uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + L::OFF_CNT);
   uint32_t* s_msk = reinterpret_cast<uint32_t*>(smem + L::OFF_MSK);
   uint32_t* s_hist = reinterpret_cast<uint32_t*>(smem + L::OFF_HIST);
@@ -171,7 +180,10 @@ __device__ void seg_sort_large(U* keys, U* scratch, int64_t n, unsigned char* sm
   uint32_t* s_local = reinterpret_cast<uint32_t*>(smem + L::OFF_LOCAL);
   uint32_t* s_gbase = reinterpret_cast<uint32_t*>(smem + L::OFF_GBASE);
   uint32_t* s_wsum = reinterpret_cast<uint32_t*>(smem + L::OFF_WSUM);
+  uint64_t* s_mbar = reinterpret_cast<uint64_t*>(smem + L::OFF_MBAR);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool staged = n >= 8 * int64_t(TILE) && (reinterpret_cast<uintptr_t>(keys) & 15) == 0 &&
+                      (reinterpret_cast<uintptr_t>(scratch) & 15) == 0;
 
   // all-digit histogram of the segment (order-independent, so one read serves every pass)
   for (int i = tid; i < P * RADIX; i += NT) s_hist[i] = 0u;
@@ -184,8 +196,18 @@ __device__ void seg_sort_large(U* keys, U* scratch, int64_t n, unsigned char* sm
   __syncthreads();
 
   const int wbase = warp * 32 * KPT;
+  const int ntiles = int((n + TILE - 1) / TILE);
   U* src = keys;
   U* dst = scratch;
+  auto issue = [&](int t) {  // one thread: tile t of src into buffer t & 1
+    const int64_t base = int64_t(t) * TILE;
+    const int64_t cnt = n - base < TILE ? n - base : TILE;
+    const uint32_t bytes = uint32_t((cnt * int64_t(sizeof(U))) & ~int64_t(15));
+    unsigned char* buf = smem + L::OFF_BUF + size_t(t & 1) * L::TILE_BYTES;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&s_mbar[t & 1], bytes);
+    if (bytes) bulk_copy_g2s(buf, src + base, bytes, &s_mbar[t & 1]);
+  };
   for (int p = 0; p < P; p++) {
     // digit starts of this pass; a pass whose keys all share one digit is the identity
     bool trivial = false;
@@ -208,14 +230,33 @@ __device__ void seg_sort_large(U* keys, U* scratch, int64_t n, unsigned char* sm
     }
     trivial = __syncthreads_or(tid < RADIX && int64_t(s_hist[p * RADIX + tid]) == n) != 0;
     if (trivial) continue;
-    for (int64_t tb = 0; tb < n; tb += TILE) {
+    if (staged && tid == 0) {
+      issue(0);
+      if (ntiles > 1) issue(1);
+    }
+    for (int t = 0; t < ntiles; t++) {
+      const int64_t tb = int64_t(t) * TILE;
       const int tile_n = int((n - tb) < TILE ? (n - tb) : TILE);
+      U* sk = reinterpret_cast<U*>(smem + L::OFF_BUF + size_t(staged ? (t & 1) : 0) * L::TILE_BYTES);
       U key[KPT];
       uint32_t pos[KPT];
+      if (staged) {
+        if (!mbar_wait_bounded(&s_mbar[t & 1], (phase >> (t & 1)) & 1u, spin_limit_ns)) {
+          if (lane == 0) atomicOr(err, uint32_t(DERR_TMA_TIMEOUT));
+        }
+        phase ^= 1u << (t & 1);
+        const int bulk_keys = int((int64_t(tile_n) * int64_t(sizeof(U))) & ~int64_t(15)) / int(sizeof(U));
 #pragma unroll
-      for (int i = 0; i < KPT; i++) {
-        const int idx = wbase + i * 32 + lane;
-        key[i] = idx < tile_n ? src[tb + idx] : U(0);
+        for (int i = 0; i < KPT; i++) {
+          const int idx = wbase + i * 32 + lane;
+          key[i] = idx < bulk_keys ? sk[idx] : (idx < tile_n ? src[tb + idx] : U(0));
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < KPT; i++) {
+          const int idx = wbase + i * 32 + lane;
+          key[i] = idx < tile_n ? src[tb + idx] : U(0);
+        }
       }
       seg_rank_tile<U, KIND, NT, KPT, MODE>(key, tile_n, 8 * p, s_cnt, s_msk, s_local, s_wsum, pos);
 #pragma unroll
@@ -231,7 +272,10 @@ __device__ void seg_sort_large(U* keys, U* scratch, int64_t n, unsigned char* sm
         else bad = true;
       }
       if (bad) atomicOr(err, uint32_t(DERR_BOUNDS));
+      // the buffer was written through the generic proxy; a bulk copy refills it
+      fence_proxy_async_smem();
       __syncthreads();
+      if (staged && tid == 0 && t + 2 < ntiles) issue(t + 2);
       // advance the running offsets by this tile's digit counts
       if (tid < RADIX) {
         const uint32_t next = tid + 1 < RADIX ? s_local[tid + 1] : uint32_t(tile_n);
@@ -239,9 +283,12 @@ __device__ void seg_sort_large(U* keys, U* scratch, int64_t n, unsigned char* sm
       }
       __syncthreads();
     }
-    U* t = src;
+    // the next pass's bulk copies read what this pass wrote through the generic proxy
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    __syncthreads();
+    U* tmp = src;
     src = dst;
-    dst = t;
+    dst = tmp;
   }
   // an odd number of executed passes leaves the result in scratch
   if (src != keys) {
@@ -383,9 +430,11 @@ __global__ void __launch_bounds__(256) seg_warp_kernel(SegParams prm) {
   }
 }
 
-// ---- block-level path: one CTA sorts one segment (in shared memory when it fits a tile,
-// else tile by tile with running offsets) -------------------------------------------------
-template <int NT, int KPT, int MODE>
+// ---- block-level path: one CTA sorts one segment ----------------------------------------
+// LARGE = false: every array fits one tile and is sorted in shared memory; LARGE = true: every
+// array is longer than a tile and is sorted tile by tile with scratch.  The plan routes each
+// array to the right one, so each kernel carries one path only (and its register count).
+template <int NT, int KPT, int MODE, bool LARGE>
 __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) segmented_sort_kernel(SegParams prm) {
   static_assert(NT >= RADIX, "one thread per digit needed");
   using L = SegSmem<NT, KPT, MODE>;
@@ -394,6 +443,13 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) segmented_sort_kernel(S
   uint32_t* s_msk = reinterpret_cast<uint32_t*>(smem + L::OFF_MSK);
   if (MODE == RANK_PEER_MASK)
     for (int i = threadIdx.x; i < L::NW * 2 * RADIX; i += NT) s_msk[i] = 0u;
+  if (LARGE && threadIdx.x == 0) {
+    uint64_t* s_mbar = reinterpret_cast<uint64_t*>(smem + L::OFF_MBAR);
+    mbar_init(&s_mbar[0], 1);
+    mbar_init(&s_mbar[1], 1);
+    fence_mbar_init();
+  }
+  uint32_t phase = 0;  // expected parity of each bulk-copy barrier (bit s: buffer s)
   uint32_t* err = prm.err;
   for (;;) {
     if (threadIdx.x == 0) *s_seg = int(atomicAdd(prm.queue, 1u));
@@ -403,33 +459,30 @@ __global__ void __launch_bounds__(NT, NT <= 256 ? 2 : 1) segmented_sort_kernel(S
     if (sidx >= prm.nsegs) break;
     const SegDesc sd = prm.segs[sidx];
     if (sd.n <= 1) continue;
-    const bool small32 = sd.n <= int64_t(NT) * KPT;
-    const bool small64 = sd.n <= int64_t(NT) * (KPT / 2);
+    const int64_t tile = sd.dtype >= 3 ? int64_t(NT) * (KPT / 2) : int64_t(NT) * KPT;
+    if ((sd.n <= tile) == LARGE) {  // the plan never routes such an array here
+      if (threadIdx.x == 0) atomicOr(err, uint32_t(DERR_BOUNDS));
+      continue;
+    }
+    auto go32 = [&](auto kind) {
+      constexpr int K = decltype(kind)::value;
+      uint32_t* k = static_cast<uint32_t*>(sd.keys);
+      if (LARGE) seg_sort_large<uint32_t, K, NT, KPT, MODE>(k, static_cast<uint32_t*>(sd.scratch), sd.n, smem, err, prm.spin_limit_ns, phase);
+      else seg_sort_small<uint32_t, K, NT, KPT, MODE>(k, int(sd.n), smem);
+    };
+    auto go64 = [&](auto kind) {
+      constexpr int K = decltype(kind)::value;
+      uint64_t* k = static_cast<uint64_t*>(sd.keys);
+      if (LARGE) seg_sort_large<uint64_t, K, NT, KPT / 2, MODE>(k, static_cast<uint64_t*>(sd.scratch), sd.n, smem, err, prm.spin_limit_ns, phase);
+      else seg_sort_small<uint64_t, K, NT, KPT / 2, MODE>(k, int(sd.n), smem);
+    };
     switch (sd.dtype) {
-      case 0:  // u32
-        if (small32) seg_sort_small<uint32_t, KIND_UNSIGNED, NT, KPT, MODE>(static_cast<uint32_t*>(sd.keys), int(sd.n), smem);
-        else seg_sort_large<uint32_t, KIND_UNSIGNED, NT, KPT, MODE>(static_cast<uint32_t*>(sd.keys), static_cast<uint32_t*>(sd.scratch), sd.n, smem, err);
-        break;
-      case 1:  // i32
-        if (small32) seg_sort_small<uint32_t, KIND_SIGNED, NT, KPT, MODE>(static_cast<uint32_t*>(sd.keys), int(sd.n), smem);
-        else seg_sort_large<uint32_t, KIND_SIGNED, NT, KPT, MODE>(static_cast<uint32_t*>(sd.keys), static_cast<uint32_t*>(sd.scratch), sd.n, smem, err);
-        break;
-      case 2:  // f32
-        if (small32) seg_sort_small<uint32_t, KIND_FLOAT, NT, KPT, MODE>(static_cast<uint32_t*>(sd.keys), int(sd.n), smem);
-        else seg_sort_large<uint32_t, KIND_FLOAT, NT, KPT, MODE>(static_cast<uint32_t*>(sd.keys), static_cast<uint32_t*>(sd.scratch), sd.n, smem, err);
-        break;
-      case 3:  // u64
-        if (small64) seg_sort_small<uint64_t, KIND_UNSIGNED, NT, KPT / 2, MODE>(static_cast<uint64_t*>(sd.keys), int(sd.n), smem);
-        else seg_sort_large<uint64_t, KIND_UNSIGNED, NT, KPT / 2, MODE>(static_cast<uint64_t*>(sd.keys), static_cast<uint64_t*>(sd.scratch), sd.n, smem, err);
-        break;
-      case 4:  // i64
-        if (small64) seg_sort_small<uint64_t, KIND_SIGNED, NT, KPT / 2, MODE>(static_cast<uint64_t*>(sd.keys), int(sd.n), smem);
-        else seg_sort_large<uint64_t, KIND_SIGNED, NT, KPT / 2, MODE>(static_cast<uint64_t*>(sd.keys), static_cast<uint64_t*>(sd.scratch), sd.n, smem, err);
-        break;
-      case 5:  // f64
-        if (small64) seg_sort_small<uint64_t, KIND_FLOAT, NT, KPT / 2, MODE>(static_cast<uint64_t*>(sd.keys), int(sd.n), smem);
-        else seg_sort_large<uint64_t, KIND_FLOAT, NT, KPT / 2, MODE>(static_cast<uint64_t*>(sd.keys), static_cast<uint64_t*>(sd.scratch), sd.n, smem, err);
-        break;
+      case 0: go32(std::integral_constant<int, KIND_UNSIGNED>()); break;
+      case 1: go32(std::integral_constant<int, KIND_SIGNED>()); break;
+      case 2: go32(std::integral_constant<int, KIND_FLOAT>()); break;
+      case 3: go64(std::integral_constant<int, KIND_UNSIGNED>()); break;
+      case 4: go64(std::integral_constant<int, KIND_SIGNED>()); break;
+      case 5: go64(std::integral_constant<int, KIND_FLOAT>()); break;
       default:
         if (threadIdx.x == 0) atomicOr(err, uint32_t(DERR_BOUNDS));
         break;

@@ -66,20 +66,23 @@ int seg_build_groups(const hpcs_seg_tuning& tuning, const hpcs_segment* segs, in
                      std::vector<SegDesc>& table, std::vector<SegGroup>& groups, size_t& scratch) {
   int rc = validate(segs, nsegs);
   if (rc != HPCS_OK) return rc;
+  // group id = 2 x variant + (tiled path)
+  constexpr int NG = 2 * SEG_NVARIANTS;
   std::vector<int> var(static_cast<size_t>(nsegs));
-  std::vector<double> group_bytes(SEG_NVARIANTS, 0.0);
+  std::vector<double> group_bytes(NG, 0.0);
   for (int64_t i = 0; i < nsegs; i++) {
     const int w = key_bytes(segs[i].dtype);
-    var[i] = tuning.variant[w == 8 ? 1 : 0][seg_class_of(segs[i].n)];
+    const int v = tuning.variant[w == 8 ? 1 : 0][seg_class_of(segs[i].n)];
+    var[i] = 2 * v + (seg_variant_large(v, segs[i].n, w) ? 1 : 0);
     group_bytes[var[i]] += double(segs[i].n) * w;
   }
   // groups in decreasing total bytes (the heaviest is launched first, on the caller's
   // stream), arrays within a group largest first
-  std::vector<int> vorder(SEG_NVARIANTS);
+  std::vector<int> vorder(NG);
   std::iota(vorder.begin(), vorder.end(), 0);
   std::stable_sort(vorder.begin(), vorder.end(), [&](int a, int b) { return group_bytes[a] > group_bytes[b]; });
-  std::vector<int> vrank(SEG_NVARIANTS);
-  for (int r = 0; r < SEG_NVARIANTS; r++) vrank[vorder[r]] = r;
+  std::vector<int> vrank(NG);
+  for (int r = 0; r < NG; r++) vrank[vorder[r]] = r;
   std::vector<int64_t> order(static_cast<size_t>(nsegs));
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
@@ -91,8 +94,11 @@ int seg_build_groups(const hpcs_seg_tuning& tuning, const hpcs_segment* segs, in
   scratch = 0;
   for (int64_t j = 0; j < nsegs; j++) {
     const hpcs_segment& sg = segs[order[j]];
-    const int v = var[order[j]];
-    if (groups.empty() || groups.back().variant != v) groups.push_back({v, int(j), 0});
+    const int gid = var[order[j]];
+    const int v = gid / 2;
+    const bool large = (gid & 1) != 0;
+    if (groups.empty() || 2 * groups.back().variant + (groups.back().large ? 1 : 0) != gid)
+      groups.push_back({v, large, int(j), 0});
     groups.back().count++;
     SegDesc& d = table[j];
     d.keys = sg.keys;
@@ -101,7 +107,7 @@ int seg_build_groups(const hpcs_seg_tuning& tuning, const hpcs_segment* segs, in
     d.pad = 0;
     d.scratch = nullptr;
     const int w = key_bytes(sg.dtype);
-    if (SEG_VARIANTS[v].kind == 1 && sg.n > seg_variant_tile_keys(v, w)) {
+    if (large) {
       d.scratch = reinterpret_cast<void*>(scratch + 1);  // offset + 1 for now (0 = none)
       scratch += (size_t(sg.n) * w + 255) / 256 * 256;
     }
@@ -128,8 +134,8 @@ int launch_groups_mode(hpcs_ctx* ctx, const SegDesc* d_desc, const std::vector<S
   }
   for (int g = 0; g < ng; g++) {
     cudaStream_t st = g == 0 ? s : ctx->seg_streams[(g - 1) % hpcs_ctx::SEG_BRANCHES];
-    if ((rc = launch_seg_variant<MODE>(ctx, groups[g].variant, d_desc + groups[g].first, groups[g].count,
-                                       d_queues + g, st)) != HPCS_OK)
+    if ((rc = launch_seg_variant<MODE>(ctx, groups[g].variant, groups[g].large, d_desc + groups[g].first,
+                                       groups[g].count, d_queues + g, st)) != HPCS_OK)
       return rc;
   }
   for (int b = 0; b < hpcs_ctx::SEG_BRANCHES && b < ng - 1; b++) {

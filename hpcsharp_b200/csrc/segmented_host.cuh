@@ -76,13 +76,14 @@ inline int seg_setup_kernel(Kernel k, int nt, size_t smem, int& blocks) {
   return HPCS_OK;
 }
 
-// One persistent launch of variant v over `nsegs` descriptors (its queue already zeroed).
+// One persistent launch of variant v over `nsegs` descriptors (its queue already zeroed);
+// `large` selects the block level's tiled path (arrays longer than the variant's tile).
 template <int MODE>
-inline int launch_seg_variant(hpcs_ctx* ctx, int v, const SegDesc* d_desc, int nsegs, uint32_t* d_queue,
-                              cudaStream_t s) {
-  static int blocks_by_dev[64][SEG_NVARIANTS] = {};
-  int& blocks = blocks_by_dev[ctx->device & 63][v];
-  SegParams prm{d_desc, nsegs, d_queue, device_error_word(ctx)};
+inline int launch_seg_variant(hpcs_ctx* ctx, int v, bool large, const SegDesc* d_desc, int nsegs,
+                              uint32_t* d_queue, cudaStream_t s) {
+  static int blocks_by_dev[64][SEG_NVARIANTS][2] = {};
+  int& blocks = blocks_by_dev[ctx->device & 63][v][large ? 1 : 0];
+  SegParams prm{d_desc, nsegs, d_queue, device_error_word(ctx), uint64_t(ctx->cfg.spin_limit_ns)};
   auto go = [&](auto k, int nt, size_t smem, int per_block) -> int {
     int rc = seg_setup_kernel(k, nt, smem, blocks);
     if (rc != HPCS_OK) return rc;
@@ -95,28 +96,39 @@ inline int launch_seg_variant(hpcs_ctx* ctx, int v, const SegDesc* d_desc, int n
     }
     return HPCS_OK;
   };
+#define HPCS_SEG_BLOCK(NTV, KPTV)                                                                          \
+  (large ? go(segmented_sort_kernel<NTV, KPTV, MODE, true>, NTV, SegSmem<NTV, KPTV, MODE>::BYTES, 1)      \
+         : go(segmented_sort_kernel<NTV, KPTV, MODE, false>, NTV, SegSmem<NTV, KPTV, MODE>::BYTES, 1))
   switch (v) {
     case 0: return go(seg_warp_kernel<4, 8, MODE>, 256, WarpSegSmem<4, MODE>::BYTES, 8);
     case 1: return go(seg_warp_kernel<8, 8, MODE>, 256, WarpSegSmem<8, MODE>::BYTES, 8);
     case 2: return go(seg_warp_kernel<16, 8, MODE>, 256, WarpSegSmem<16, MODE>::BYTES, 8);
     case 3: return go(seg_warp_kernel<8, 4, MODE>, 256, WarpSegSmem<8, MODE>::BYTES, 8);
     case 4: return go(seg_warp_kernel<16, 4, MODE>, 256, WarpSegSmem<16, MODE>::BYTES, 8);
-    case 5: return go(segmented_sort_kernel<256, 8, MODE>, 256, SegSmem<256, 8, MODE>::BYTES, 1);
-    case 6: return go(segmented_sort_kernel<256, 16, MODE>, 256, SegSmem<256, 16, MODE>::BYTES, 1);
-    case 7: return go(segmented_sort_kernel<512, 8, MODE>, 512, SegSmem<512, 8, MODE>::BYTES, 1);
-    case 8: return go(segmented_sort_kernel<512, 16, MODE>, 512, SegSmem<512, 16, MODE>::BYTES, 1);
-    case 9: return go(segmented_sort_kernel<512, 32, MODE>, 512, SegSmem<512, 32, MODE>::BYTES, 1);
+    case 5: return HPCS_SEG_BLOCK(256, 8);
+    case 6: return HPCS_SEG_BLOCK(256, 16);
+    case 7: return HPCS_SEG_BLOCK(512, 8);
+    case 8: return HPCS_SEG_BLOCK(512, 16);
+    case 9: return HPCS_SEG_BLOCK(512, 32);
     case 10: return go(seg_warp_kernel<32, 8, MODE>, 256, WarpSegSmem<32, MODE>::BYTES, 8);
     default: return fail(HPCS_ERR_RANGE, "unknown segmented-sort variant");
   }
+#undef HPCS_SEG_BLOCK
 }
 
-// A descriptor table grouped by variant: group g covers [first, first + count) and uses queue g.
+// A descriptor table grouped by (variant, path): group g covers [first, first + count) and
+// uses queue g; `large` marks block-level arrays longer than the variant's tile.
 struct SegGroup {
   int variant;
+  bool large;
   int first;
   int count;
 };
+
+// Whether variant v sorts an array of n keys of width w with its tiled (scratch) path.
+inline bool seg_variant_large(int v, int64_t n, int key_bytes) {
+  return SEG_VARIANTS[v].kind == 1 && n > seg_variant_tile_keys(v, key_bytes);
+}
 
 // Orders the descriptors by (variant, bytes descending), fills `groups`, and returns through
 // `scratch` the bytes of scratch the block-level arrays longer than one tile need (their

@@ -149,8 +149,7 @@ int coalesced_variant(const hpcs_seg_tuning& t, const hpcs_request& r) {
   return t.variant[dtype_bytes(r.dtype) == 8 ? 1 : 0][seg_class_of(r.n)];
 }
 bool coalesced_needs_scratch(const hpcs_seg_tuning& t, const hpcs_request& r) {
-  const int v = coalesced_variant(t, r);
-  return SEG_VARIANTS[v].kind == 1 && r.n > seg_variant_tile_keys(v, dtype_bytes(r.dtype));
+  return seg_variant_large(coalesced_variant(t, r), r.n, dtype_bytes(r.dtype));
 }
 
 // Bytes of a coalesced request: its keys, plus segment scratch if its variant needs it.
@@ -302,8 +301,11 @@ void launch_batch(hpcs_server* sv) {
   uint32_t* d_queues = reinterpret_cast<uint32_t*>(sv->arena_base + sv->batch_meta_off + n * sizeof(SegDesc));
   std::vector<size_t> order(n);
   for (size_t i = 0; i < n; i++) order[i] = i;
+  auto gid = [&](const hpcs_request& r) {
+    return 2 * coalesced_variant(c->seg_tuning, r) + (coalesced_needs_scratch(c->seg_tuning, r) ? 1 : 0);
+  };
   std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
-    const int va = coalesced_variant(c->seg_tuning, sv->batch[a]->r), vb = coalesced_variant(c->seg_tuning, sv->batch[b]->r);
+    const int va = gid(sv->batch[a]->r), vb = gid(sv->batch[b]->r);
     if (va != vb) return va < vb;
     return sv->batch[a]->r.n * dtype_bytes(sv->batch[a]->r.dtype) > sv->batch[b]->r.n * dtype_bytes(sv->batch[b]->r.dtype);
   });
@@ -312,7 +314,9 @@ void launch_batch(hpcs_server* sv) {
     Req* q = sv->batch[order[j]];
     const int w = dtype_bytes(q->r.dtype);
     const int v = coalesced_variant(c->seg_tuning, q->r);
-    if (groups.empty() || groups.back().variant != v) groups.push_back({v, int(j), 0});
+    const bool large = coalesced_needs_scratch(c->seg_tuning, q->r);
+    if (groups.empty() || groups.back().variant != v || groups.back().large != large)
+      groups.push_back({v, large, int(j), 0});
     groups.back().count++;
     unsigned char* keys = sv->arena_base + q->off;
     SegDesc& d = sv->host_table[j];
