@@ -270,7 +270,7 @@ int check_select_args(hpcs_ctx* ctx, const void* a, int64_t n, int64_t k) {
   // SelectTopK(a, k): length must be positive and k a valid index (SelectionTopKRadix.cs:164-167;
   // k == Length passes the reference's check but then indexes past its bins).
   if (n <= 0) return fail(HPCS_ERR_RANGE, "array length is invalid");
-  if (n > HPCS_MAX_KEYS) return fail(HPCS_ERR_RANGE, "length exceeds HPCS_MAX_KEYS");
+  if (n > HPCS_MAX_SEGMENT_KEYS) return fail(HPCS_ERR_RANGE, "length exceeds HPCS_MAX_SEGMENT_KEYS");
   if (k < 0 || k >= n) return fail(HPCS_ERR_RANGE, "k must be in [0, length)");
   return HPCS_OK;
 }
@@ -315,7 +315,7 @@ int select_topk_dev(hpcs_ctx* ctx, T* a, int64_t n, int64_t k, void* stream) {
 int check_topk_args(hpcs_ctx* ctx, const void* in, const void* out, int64_t n, int64_t k) {
   if (!ctx) return fail(HPCS_ERR_NULL, "ctx is NULL");
   if (!in || !out) return fail(HPCS_ERR_NULL, "array is NULL");
-  if (n < 0 || n > HPCS_MAX_KEYS) return fail(HPCS_ERR_RANGE, "length out of range");
+  if (n < 0 || n > HPCS_MAX_SEGMENT_KEYS) return fail(HPCS_ERR_RANGE, "length out of range");
   if (k < 0 || k > n) return fail(HPCS_ERR_RANGE, "k must be in [0, length]");
   return HPCS_OK;
 }

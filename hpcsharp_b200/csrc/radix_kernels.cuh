@@ -39,7 +39,8 @@ constexpr uint32_t ST_AGGREGATE = 1u << 30;  // tile-local count only
 constexpr uint32_t ST_PREFIX = 2u << 30;     // inclusive prefix over tiles 0..t
 constexpr uint32_t ST_FLAGS = 3u << 30;
 constexpr uint32_t ST_VALUE = (1u << 30) - 1;
-constexpr int64_t MAX_KEYS_PER_SORT = (int64_t(1) << 30) - 1;
+constexpr int64_t MAX_KEYS_PER_SORT = (int64_t(1) << 31) - 1;     // chunked passes: 32-bit positions
+constexpr int64_t MAX_KEYS_LOOKBACK = (int64_t(1) << 30) - 1;     // look-back: 30-bit prefixes
 // Predecessor status words read per look-back step.
 #ifndef HPCS_LB_WINDOW
 #define HPCS_LB_WINDOW 8

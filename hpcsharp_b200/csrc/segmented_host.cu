@@ -31,7 +31,7 @@ int validate(const hpcs_segment* segs, int64_t nsegs) {
   if (!segs && nsegs > 0) return fail(HPCS_ERR_NULL, "segments is NULL");
   if (nsegs < 0 || nsegs > (int64_t(1) << 31) - 1) return fail(HPCS_ERR_RANGE, "segment count out of range");
   for (int64_t i = 0; i < nsegs; i++) {
-    if (segs[i].n < 0 || segs[i].n > HPCS_MAX_KEYS) return fail(HPCS_ERR_RANGE, "segment length out of range");
+    if (segs[i].n < 0 || segs[i].n > HPCS_MAX_SEGMENT_KEYS) return fail(HPCS_ERR_RANGE, "segment length out of range");
     if (segs[i].n > 0 && !segs[i].keys) return fail(HPCS_ERR_NULL, "segment keys is NULL");
     if (segs[i].dtype < HPCS_U32 || segs[i].dtype > HPCS_F64) return fail(HPCS_ERR_UNSUPPORTED, "unknown dtype");
   }

@@ -436,7 +436,7 @@ int check_request(hpcs_server* sv, const hpcs_request* r) {
   if (!r || !r->input || !r->output) return fail(HPCS_ERR_NULL, "request, input or output is NULL");
   if (r->op != HPCS_OP_SORT && r->op != HPCS_OP_TOPK) return fail(HPCS_ERR_UNSUPPORTED, "unknown op");
   if (r->dtype < HPCS_U32 || r->dtype > HPCS_F64) return fail(HPCS_ERR_UNSUPPORTED, "unknown dtype");
-  if (r->n <= 0 || r->n > HPCS_MAX_KEYS) return fail(HPCS_ERR_RANGE, "n out of range");
+  if (r->n <= 0 || r->n > HPCS_MAX_SEGMENT_KEYS) return fail(HPCS_ERR_RANGE, "n out of range");
   if (r->op == HPCS_OP_TOPK && (r->k < 0 || r->k > r->n)) return fail(HPCS_ERR_RANGE, "k must be in [0, n]");
   const size_t need = r->n <= sv->cfg.coalesce_max_keys ? coalesced_bytes(sv->bctx->seg_tuning, *r) + 256 : slot_layout(*r).total;
   if (need > sv->arena.size()) return fail(HPCS_ERR_OOM, "request larger than the server's HBM budget");

@@ -331,6 +331,8 @@ int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t
   constexpr bool PAIRS = !std::is_same<V, NoValue>::value;
   if (n <= 1) return HPCS_OK;
   if (n > MAX_KEYS_PER_SORT) return fail(HPCS_ERR_RANGE, "n exceeds HPCS_MAX_KEYS");
+  if (ctx->cfg.pass_scheme == HPCS_PASSES_LOOKBACK && n > MAX_KEYS_LOOKBACK)
+    return fail(HPCS_ERR_RANGE, "look-back passes take at most 2^30 - 1 keys (30-bit prefixes)");
   const bool lookback = ctx->cfg.pass_scheme == HPCS_PASSES_LOOKBACK ||
                         (ctx->cfg.pass_scheme != HPCS_PASSES_CHUNKED && n < ChunkMinKeys<U, V>::value);
   const bool ordered = ctx->rank_mode == RANK_ORDERED_ATOMIC;

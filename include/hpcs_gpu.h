@@ -14,7 +14,8 @@
  *   - bad length / k / l,r -> HPCS_ERR_RANGE (reference: ArgumentOutOfRangeException,
  *                                            SelectionTopKRadix.cs:146-149, :164-167)
  *   - n == 0 returns HPCS_OK at once (RadixSortLsdParallel.cs:175-176).
- *   - One call sorts at most HPCS_MAX_KEYS keys.
+ *   - One sort, pairs sort or histogram call takes at most HPCS_MAX_KEYS keys; a segmented
+ *     array, a served request or a select / top-k call at most HPCS_MAX_SEGMENT_KEYS.
  *   - Host-array functions (no suffix) are synchronous: they copy the caller's array to
  *     the GPU, sort, copy back into the same array and return.  The result is the
  *     reference's in-place result (the caller's array sorted, RadixSortLsdParallel.cs:227-231).
@@ -37,7 +38,10 @@ extern "C" {
 #endif
 
 #define HPCS_ABI_VERSION 1
-#define HPCS_MAX_KEYS ((int64_t)1073741823) /* 2^30 - 1 keys per call */
+#define HPCS_MAX_KEYS ((int64_t)2147483647) /* 2^31 - 1 keys per sort, pairs sort or histogram
+                                                call: the longest .NET array */
+#define HPCS_MAX_SEGMENT_KEYS ((int64_t)1073741823) /* 2^30 - 1 keys per segmented array,
+                                                       served request or select / top-k call */
 
 typedef enum hpcs_status {
   HPCS_OK = 0,
@@ -190,7 +194,7 @@ int hpcs_histogram_byte_components_dev(hpcs_ctx* ctx, int dtype, const void* a, 
  * No reference counterpart (HPCsharp sorts one array per call): many independent arrays of
  * mixed length and dtype sorted in one persistent launch, each with exactly the plain sort's
  * result (stable, ascending, same order transforms).  Keys are device pointers, sorted in
- * place; each array's n <= HPCS_MAX_KEYS. */
+ * place; each array's n <= HPCS_MAX_SEGMENT_KEYS. */
 typedef struct hpcs_segment {
   void* keys;      /* device pointer */
   int64_t n;

@@ -68,3 +68,36 @@ def test_pairs_at_scale(ctx, dt, n, gen):
         assert int(same.sum()) > n // 2  # Zipf duplicates are heavy
     del keys, orig, items, idx, o, same
     torch.cuda.empty_cache()
+
+
+def test_sort_beyond_2_to_30_keys(ctx):
+    """A .NET array may hold up to 2^31 - 1 keys; the chunked passes use 32-bit positions, so a
+    plain sort and a pairs sort of more than 2^30 keys work (sorted, a permutation, stable)."""
+    import torch
+
+    n = (1 << 30) + 4097
+    a = datagen.u32_uniform(n, 5)
+    t = to_dev(a)
+    del a
+    before = checksum_dev(t)
+    ctx.sort_dev(t, dtype="u32", stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    assert is_sorted_dev(t, "u32")
+    assert checksum_dev(t) == before
+    # pairs: keys with heavy duplicates, items = input positions
+    keys = (t[:n] & 0xFFFF).contiguous()  # a sorted-then-masked permutation: many equal keys
+    orig = keys.clone()
+    del t
+    items = torch.arange(n, dtype=torch.int32, device="cuda")
+    ctx.sort_pairs_dev(keys, items, dtype="u32", stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    assert is_sorted_dev(keys, "u32")
+    idx = items.to(torch.int64)
+    assert int(idx.sum()) == n * (n - 1) // 2
+    assert torch.equal(orig[idx], keys)
+    same = keys[1:] == keys[:-1]
+    assert bool((idx[1:][same] > idx[:-1][same]).all())
+    del keys, orig, items, idx, same
+    torch.cuda.empty_cache()

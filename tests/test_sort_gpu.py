@@ -160,7 +160,9 @@ def test_argument_errors(ctx):
     assert lib.hpcs_sort_u32(ctx.handle, None, 10) == native.HPCS_ERR_NULL
     assert lib.hpcs_sort_u32(ctx.handle, a.ctypes.data, -1) == native.HPCS_ERR_RANGE
     assert lib.hpcs_sort_u32(ctx.handle, a.ctypes.data, 0) == native.HPCS_OK
-    assert lib.hpcs_sort_u32(ctx.handle, a.ctypes.data, (1 << 30)) == native.HPCS_ERR_RANGE
+    assert lib.hpcs_sort_u32(ctx.handle, a.ctypes.data, (1 << 31)) == native.HPCS_ERR_RANGE
+    # select / top-k keep the 2^30 - 1 limit (checked before any copy)
+    assert lib.hpcs_select_topk_u32(ctx.handle, a.ctypes.data, (1 << 30), 0) == native.HPCS_ERR_RANGE
     with pytest.raises(native.ArgumentNullException):
         algorithm.SortRadixPar(None)
 
