@@ -15,6 +15,8 @@ Reference surface (paths relative to the HPCsharp project root):
   ParallelAlgorithm.HistogramByteComponentsPar(T[], int l, int r, ...)  HistogramParallel.cs:214, :416, :547, :617
   Algorithm.SelectTopK(this uint[], int k) / (a, start, length, k)     SelectionTopKRadix.cs:160, :142
   Algorithm.SortRadixMsd(this float[]/double[]/...)                       RadixSortMsd.cs:1563-1610
+  Algorithm.SortCounting[InPlace[Func]](this byte[]/sbyte[]/ushort[]/short[]) CountingSort.cs:23-165
+  ParallelAlgorithm.SortCounting[InPlace[Func]]Par(...)                   CountingSortParallel.cs:22-99
   Algorithm.SelectRadix(this uint[]/ulong[], k or int[] k [, start, length])
                                                                        SelectionRadix.cs:236-435
 
@@ -184,3 +186,28 @@ def SortRadixMsd(arrayToBeSorted: np.ndarray) -> np.ndarray:
     identical result (equal keys are identical bit patterns, so stability is unobservable)."""
     _require(arrayToBeSorted, "arrayToBeSorted")
     return default_context().sort(arrayToBeSorted)
+
+
+def SortCountingInPlace(arrayToSort: np.ndarray) -> None:
+    """SortCountingInPlace(this byte[]/sbyte[]/ushort[]/short[]) CountingSort.cs:41, :78, :115,
+    :152: in place, ascending, by the GPU counting sort (one histogram read, one fill)."""
+    _require(arrayToSort, "arrayToSort")
+    default_context().sort(arrayToSort)
+
+
+def SortCountingInPlaceFunc(arrayToSort: np.ndarray) -> np.ndarray:
+    SortCountingInPlace(arrayToSort)
+    return arrayToSort
+
+
+def SortCounting(inputArray: np.ndarray) -> np.ndarray:
+    """SortCounting(this byte[]/...) CountingSort.cs:23: a new sorted array."""
+    _require(inputArray, "inputArray")
+    out = np.array(inputArray, copy=True)
+    default_context().sort(out)
+    return out
+
+
+SortCountingPar = SortCounting
+SortCountingInPlacePar = SortCountingInPlace
+SortCountingInPlaceFuncPar = SortCountingInPlaceFunc

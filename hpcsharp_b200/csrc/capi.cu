@@ -7,6 +7,7 @@
 
 #include "../../include/hpcs_gpu.h"
 #include "sort_host.cuh"
+#include "counting.cuh"
 #include "segmented_host.cuh"
 #include "topk_host.cuh"
 
@@ -182,6 +183,69 @@ int sort_dev(hpcs_ctx* ctx, T* keys, int64_t n, void* stream) {
   cudaStream_t s = pick_stream(ctx, stream);
   if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
   return enqueue_sort<U, KIND, NoValue>(ctx, reinterpret_cast<U*>(keys), nullptr, n, s);
+}
+
+// Counting sort of 8/16-bit keys in device memory (histogram, scan, fill), in place.
+template <class U>
+int enqueue_count_sort(hpcs_ctx* ctx, U* d, int64_t n, uint32_t flip, cudaStream_t s) {
+  constexpr int BINS = CountTraits<U>::BINS;
+  int rc;
+  if ((rc = ensure(ctx, ctx->counts, size_t(BINS) * 4)) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->aux2, size_t(BINS + 1) * 8)) != HPCS_OK) return rc;
+  uint32_t* counts = static_cast<uint32_t*>(ctx->counts.ptr);
+  int64_t* starts = static_cast<int64_t*>(ctx->aux2.ptr);
+  const size_t smem = BINS == 256 ? size_t(256) * 32 * 4 : size_t(BINS / 2) * 4;
+  auto kh = count_hist_kernel<U>;
+  static int attr_set[64] = {0};
+  if (!attr_set[ctx->device & 63]) {
+    HPCS_CUDA(cudaFuncSetAttribute(kh, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    attr_set[ctx->device & 63] = 1;
+  }
+  HPCS_CUDA(cudaMemsetAsync(counts, 0, size_t(BINS) * 4, s));
+  const int64_t want = (n + int64_t(COUNT_NT) * 16 - 1) / (int64_t(COUNT_NT) * 16);
+  const int hgrid = int(want < 1 ? 1 : (want > ctx->sms ? ctx->sms : want));
+  {
+    KernelTimer kt(ctx, s, HPCS_K_HISTOGRAM);
+    kh<<<hgrid, COUNT_NT, smem, s>>>(d, n, flip, counts);
+    HPCS_CUDA(cudaGetLastError());
+  }
+  count_scan_kernel<BINS><<<1, COUNT_NT, 0, s>>>(counts, starts);
+  HPCS_CUDA(cudaGetLastError());
+  const int64_t vecs = n / (16 / int64_t(sizeof(U))) + 1;
+  const int64_t fwant = (vecs + 255) / 256;
+  const int fgrid = int(fwant > int64_t(ctx->sms) * 16 ? int64_t(ctx->sms) * 16 : fwant);
+  {
+    KernelTimer kt(ctx, s, HPCS_K_FINALIZE);
+    count_fill_kernel<U><<<fgrid, 256, 0, s>>>(d, n, starts, flip);
+    HPCS_CUDA(cudaGetLastError());
+  }
+  return HPCS_OK;
+}
+
+template <class T, class U>
+int count_sort_host(hpcs_ctx* ctx, T* keys, int64_t n, uint32_t flip) {
+  int rc = check_common(ctx, keys, n);
+  if (rc != HPCS_OK || n == 0) return rc;
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = ctx->stream;
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->keys_a, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
+  U* d = static_cast<U*>(ctx->keys_a.ptr);
+  HPCS_CUDA(cudaMemcpyAsync(d, keys, size_t(n) * sizeof(U), cudaMemcpyHostToDevice, s));
+  if ((rc = enqueue_count_sort<U>(ctx, d, n, flip, s)) != HPCS_OK) return rc;
+  HPCS_CUDA(cudaMemcpyAsync(keys, d, size_t(n) * sizeof(U), cudaMemcpyDeviceToHost, s));
+  HPCS_CUDA(cudaStreamSynchronize(s));
+  return check_device_errors(ctx);
+}
+
+template <class T, class U>
+int count_sort_dev(hpcs_ctx* ctx, T* keys, int64_t n, uint32_t flip, void* stream) {
+  int rc = check_common(ctx, keys, n);
+  if (rc != HPCS_OK || n == 0) return rc;
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = pick_stream(ctx, stream);
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  return enqueue_count_sort<U>(ctx, reinterpret_cast<U*>(keys), n, flip, s);
 }
 
 template <class T, class U, int KIND>
@@ -587,6 +651,19 @@ int hpcs_histogram_byte_components_i64(hpcs_ctx* c, const int64_t* a, int64_t l,
 }
 int hpcs_histogram_byte_components_f64(hpcs_ctx* c, const double* a, int64_t l, int64_t r, uint32_t* o) {
   return histogram_host<double, uint64_t, KIND_FLOAT>(c, a, l, r, o);
+}
+
+int hpcs_sort_u8(hpcs_ctx* c, uint8_t* k, int64_t n) { return count_sort_host<uint8_t, uint8_t>(c, k, n, 0u); }
+int hpcs_sort_i8(hpcs_ctx* c, int8_t* k, int64_t n) { return count_sort_host<int8_t, uint8_t>(c, k, n, 0x80u); }
+int hpcs_sort_u16(hpcs_ctx* c, uint16_t* k, int64_t n) { return count_sort_host<uint16_t, uint16_t>(c, k, n, 0u); }
+int hpcs_sort_i16(hpcs_ctx* c, int16_t* k, int64_t n) { return count_sort_host<int16_t, uint16_t>(c, k, n, 0x8000u); }
+int hpcs_sort_u8_dev(hpcs_ctx* c, uint8_t* k, int64_t n, void* s) { return count_sort_dev<uint8_t, uint8_t>(c, k, n, 0u, s); }
+int hpcs_sort_i8_dev(hpcs_ctx* c, int8_t* k, int64_t n, void* s) { return count_sort_dev<int8_t, uint8_t>(c, k, n, 0x80u, s); }
+int hpcs_sort_u16_dev(hpcs_ctx* c, uint16_t* k, int64_t n, void* s) {
+  return count_sort_dev<uint16_t, uint16_t>(c, k, n, 0u, s);
+}
+int hpcs_sort_i16_dev(hpcs_ctx* c, int16_t* k, int64_t n, void* s) {
+  return count_sort_dev<int16_t, uint16_t>(c, k, n, 0x8000u, s);
 }
 
 #define HPCS_TOPK_EXPORTS(NAME, T, U, KIND)                                                          \

@@ -32,11 +32,19 @@ CT_OF = {"u32": C.c_uint32, "i32": C.c_int32, "f32": C.c_float, "u64": C.c_uint6
          "f64": C.c_double}
 
 
-def dtype_name(arr_dtype) -> str:
+# 8- and 16-bit keys: sorted by the counting sort (plain sorts only)
+COUNT_NP_OF = {"u8": np.uint8, "i8": np.int8, "u16": np.uint16, "i16": np.int16}
+
+
+def dtype_name(arr_dtype, counting: bool = False) -> str:
     dt = np.dtype(arr_dtype)
     for k, v in NP_OF.items():
         if np.dtype(v) == dt:
             return k
+    if counting:
+        for k, v in COUNT_NP_OF.items():
+            if np.dtype(v) == dt:
+                return k
     raise TypeError(f"unsupported key dtype {dt}")
 
 
@@ -148,6 +156,9 @@ def _declare(lib) -> None:
         getattr(lib, f"hpcs_topk_largest_{t}").argtypes = [P, P, I64, I64, P]
         getattr(lib, f"hpcs_topk_largest_{t}_dev").argtypes = [P, P, I64, I64, P, P]
     lib.hpcs_histogram_byte_components_dev.argtypes = [P, I32, P, I64, P, P]
+    for t in COUNT_NP_OF:
+        getattr(lib, f"hpcs_sort_{t}").argtypes = [P, P, I64]
+        getattr(lib, f"hpcs_sort_{t}_dev").argtypes = [P, P, I64, P]
     lib.hpcs_ctx_profile_enable.argtypes = [P, I32]
     lib.hpcs_ctx_profile_read.argtypes = [P, C.POINTER(HpcsProfile)]
     lib.hpcs_ctx_trace_tiles.argtypes = [P, P, I32, I32]
@@ -297,7 +308,7 @@ class Context:
 
     # ---- host arrays (synchronous, in place) ----
     def sort(self, a: np.ndarray) -> np.ndarray:
-        t = dtype_name(a.dtype)
+        t = dtype_name(a.dtype, counting=True)
         check(getattr(self.lib, f"hpcs_sort_{t}")(self.handle, _ptr(a), a.size))
         return a
 

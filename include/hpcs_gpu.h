@@ -190,6 +190,19 @@ int hpcs_histogram_byte_components_f64(hpcs_ctx* ctx, const double* a, int64_t l
 int hpcs_histogram_byte_components_dev(hpcs_ctx* ctx, int dtype, const void* a, int64_t n, uint32_t* counts,
                                        void* stream);
 
+/* ---- counting sort of 8- and 16-bit keys ----------------------------------------------
+ * SortCountingInPlace(this byte[] / sbyte[] / ushort[] / short[]) CountingSort.cs:41, :78,
+ * :115, :152 and SortCountingInPlacePar CountingSortParallel.cs:41: in place, ascending
+ * (signed keys by value).  One histogram read, a scan of the 2^8 / 2^16 counts, one fill. */
+int hpcs_sort_u8(hpcs_ctx* ctx, uint8_t* keys, int64_t n);
+int hpcs_sort_i8(hpcs_ctx* ctx, int8_t* keys, int64_t n);
+int hpcs_sort_u16(hpcs_ctx* ctx, uint16_t* keys, int64_t n);
+int hpcs_sort_i16(hpcs_ctx* ctx, int16_t* keys, int64_t n);
+int hpcs_sort_u8_dev(hpcs_ctx* ctx, uint8_t* keys, int64_t n, void* stream);
+int hpcs_sort_i8_dev(hpcs_ctx* ctx, int8_t* keys, int64_t n, void* stream);
+int hpcs_sort_u16_dev(hpcs_ctx* ctx, uint16_t* keys, int64_t n, void* stream);
+int hpcs_sort_i16_dev(hpcs_ctx* ctx, int16_t* keys, int64_t n, void* stream);
+
 /* ---- batched segmented sort ------------------------------------------------------------
  * No reference counterpart (HPCsharp sorts one array per call): many independent arrays of
  * mixed length and dtype sorted in one persistent launch, each with exactly the plain sort's

@@ -261,3 +261,36 @@ def test_sort_radix_msd_alias(ctx, orc, dt):
     want = oracle_sorted(orc, a)
     got = algorithm.SortRadixMsd(a.copy())
     assert_same_bits(got, want)
+
+
+@pytest.mark.parametrize("dt", [np.uint8, np.int8, np.uint16, np.int16])
+@pytest.mark.parametrize("n", [1, 15, 16, 17, 4099, 1_000_003, 40_000_001])
+def test_counting_sort_8_16_bit(ctx, dt, n):
+    """SortCountingInPlace / SortCounting for byte, sbyte, ushort and short keys: equal to a
+    stable sort by value (uniform and skewed values, ragged 16-byte tails)."""
+    rng = np.random.default_rng(n)
+    info = np.iinfo(dt)
+    a = rng.integers(info.min, int(info.max) + 1, size=n, dtype=np.int64).astype(dt)
+    if n > 1000:
+        a[: n // 3] = dt(7)  # one value holds a third of the keys
+        rng.shuffle(a)
+    want = np.sort(a, kind="stable")
+    got = algorithm.SortCounting(a)
+    assert np.array_equal(got, want)
+    b = a.copy()
+    algorithm.SortCountingInPlace(b)
+    assert np.array_equal(b, want)
+
+
+def test_counting_sort_device_unaligned(ctx):
+    import torch
+
+    a = np.random.default_rng(3).integers(0, 65536, size=100_003, dtype=np.int64).astype(np.uint16)
+    t = torch.from_numpy(a.view(np.int16).copy()).cuda()
+    big = torch.zeros(a.size + 3, dtype=torch.int16, device="cuda")
+    big[3:].copy_(t)
+    lib = native.load()
+    native.check(lib.hpcs_sort_u16_dev(ctx.handle, big.data_ptr() + 6, a.size, torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    ctx.synchronize()
+    assert np.array_equal(big[3:].cpu().numpy().view(np.uint16), np.sort(a))
