@@ -52,10 +52,13 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps (capped at 20)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "served", "configs"],
+    ap.add_argument("--workload", default="plain",
+                    choices=["plain", "batched", "served", "configs", "sharded"],
                     help="plain: the 2^28-key sort (headline); batched: 65,536 mixed arrays; "
                          "served: Poisson sort/top-k requests swept to saturation; configs: every "
-                         "plain-sort and pairs configuration, device-resident")
+                         "plain-sort and pairs configuration, device-resident; sharded: one array of "
+                         "--n keys per rank sorted across the ranks (partition, NCCL all-to-all, "
+                         "local sort, rebalance)")
     ap.add_argument("--requests", type=int, default=120, help="served: requests per arrival rate")
     ap.add_argument("--loads", default="0.25,0.5,1,2,4,8,16",
                     help="served: offered loads, as multiples of the plain form's capacity")
@@ -688,6 +691,91 @@ def run_configs(args, rank: int, world: int, local_rank: int):
                       "steps": steps, "rows": rows}), flush=True)
 
 
+def run_sharded(args, rank: int, world: int, local_rank: int):
+    """The sharded sort of one array of world x n keys (n per rank, weak scaling): every step
+    partitions, exchanges (NCCL all-to-all), sorts and rebalances; CUDA events on the current
+    stream around each step (host synchronisations of the exchange sizes included), max over
+    ranks.  Also times the partition kernel alone into 8 parts (its roofline: one read and one
+    write of the keys per launch)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from hpcsharp_b200 import native, replicas, sharded
+
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    if "MASTER_ADDR" not in os.environ:
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(29400 + os.getpid() % 500))
+    dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120),
+                            device_id=torch.device(f"cuda:{dev}"))
+    n, dtype = args.n, args.dtype
+    w = np.dtype(native.NP_OF[dtype]).itemsize
+    host = gen_keys(dtype, n, seed=1 + rank)
+    keys = torch.from_numpy(host.view({4: np.int32, 8: np.int64}[w])).to(f"cuda:{dev}")
+    ctx = native.Context(dev)
+    ops = sharded.DeviceOps(ctx, dtype)
+    for _ in range(max(3, args.warmup)):
+        out, _ = sharded.sort_sharded(keys, ops=ops)
+    torch.cuda.synchronize()
+    steps = max(1, min(args.steps, 10))
+    ctx.profile(True)
+    tot = 0.0
+    for _ in range(steps):
+        dist.barrier()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        out, _ = sharded.sort_sharded(keys, ops=ops)
+        b.record()
+        torch.cuda.synchronize()
+        tot += a.elapsed_time(b)
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    tot = replicas.max_over_ranks(tot, device=f"cuda:{dev}")
+    ok = _in_order(out[:1 << 20].cpu().numpy().view(host.dtype)) and out.numel() == n
+    # the partition kernel alone, 8 parts, splitters from a sorted sample of the keys
+    parts = 8
+    stream = native.torch_stream()
+    samp = keys[torch.randint(0, n, (4096,), device=f"cuda:{dev}")].contiguous()
+    idx = torch.arange(4096, dtype=torch.int32, device=f"cuda:{dev}")
+    ctx.sort_pairs_dev(samp, idx, dtype=dtype, stream=stream)
+    pick = torch.tensor([(j * 4096) // parts for j in range(1, parts)], device=f"cuda:{dev}")
+    sk = samp[pick].contiguous()
+    sg = torch.zeros(parts - 1, dtype=torch.int64, device=f"cuda:{dev}")
+    ko = torch.empty_like(keys)
+    cnt = torch.empty(parts, dtype=torch.int64, device=f"cuda:{dev}")
+    for _ in range(3):
+        ctx.shard_partition_dev(keys, None, 0, sk, sg, parts, ko, None, cnt, dtype=dtype, stream=stream)
+    torch.cuda.synchronize()
+    pt = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        ctx.shard_partition_dev(keys, None, 0, sk, sg, parts, ko, None, cnt, dtype=dtype, stream=stream)
+        b.record()
+        torch.cuda.synchronize()
+        pt.append(a.elapsed_time(b))
+    part_ms = statistics.median(pt)
+    hbm, peak_kind = peaks()
+    part_gbs = 2.0 * n * w / (part_ms / 1e3) / 1e9
+    dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "Gkeys/s, sharded sort of one array across ranks", "workload": "sharded",
+            "value": round(n * world * steps / (tot / 1e3) / 1e9, 4), "unit": UNIT, "n_gpus": world,
+            "steps": steps, "ms_per_step": round(tot / steps, 4), "scaling": "weak", "dtype": dtype,
+            "config": {"keys_per_rank": n, "dtype": dtype, "balance": True, "samples_per_rank": 1024},
+            "sorted": bool(ok),
+            "kernels_ms_per_step": {k: round(v[1] / steps, 4) for k, v in prof.items() if v[0]},
+            "partition_8_parts": {"ms": round(part_ms, 4), "achieved_gbs": round(part_gbs, 1),
+                                  "algorithmic_bytes": 2 * n * w, "peak": hbm, "peak_kind": peak_kind,
+                                  "frac": round(part_gbs / hbm, 4), "counts": cnt.cpu().tolist()},
+        }), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -704,6 +792,9 @@ def main():
         return
     if args.workload == "configs":
         run_configs(args, rank, world, local_rank)
+        return
+    if args.workload == "sharded":
+        run_sharded(args, rank, world, local_rank)
         return
     run_ours(args, rank, world, local_rank)
 

@@ -10,6 +10,7 @@
 #include "counting.cuh"
 #include "segmented_host.cuh"
 #include "topk_host.cuh"
+#include "shard.cuh"
 
 namespace hpcs {
 
@@ -412,6 +413,54 @@ int topk_largest_host(hpcs_ctx* ctx, const T* in, int64_t n, int64_t k, T* out) 
   return check_device_errors(ctx);
 }
 
+// Count, scan and scatter of one shard into `parts` parts (shard.cuh).  Three CTAs per SM
+// (the scatter kernel's 80 registers x 256 threads allow three), each a contiguous range of
+// whole tiles; both passes use the same ranges.
+template <class U, int KIND>
+int enqueue_shard_partition(hpcs_ctx* ctx, const U* keys, const uint32_t* items, int64_t n, int64_t gpos0,
+                            const U* split_keys, const int64_t* split_gpos, int parts, U* keys_out,
+                            uint32_t* items_out, int64_t* counts_out, cudaStream_t s) {
+  if (n == 0) {
+    HPCS_CUDA(cudaMemsetAsync(counts_out, 0, size_t(parts) * 8, s));
+    return HPCS_OK;
+  }
+  const int64_t tiles = (n + SHARD_TILE - 1) / SHARD_TILE;
+  const int64_t cap = int64_t(ctx->sms) * 3;
+  const int grid = int(tiles < cap ? tiles : cap);
+  const int64_t per_cta = (tiles + grid - 1) / grid * SHARD_TILE;
+  int rc;
+  if ((rc = ensure(ctx, ctx->aux0, size_t(grid) * parts * 4)) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->aux1, size_t(grid) * parts * 8)) != HPCS_OK) return rc;
+  uint32_t* cta_counts = static_cast<uint32_t*>(ctx->aux0.ptr);
+  int64_t* cta_offsets = static_cast<int64_t*>(ctx->aux1.ptr);
+  KernelTimer kt(ctx, s, HPCS_K_SHARD);
+  shard_count_kernel<U, KIND><<<grid, SHARD_NT, 0, s>>>(keys, n, per_cta, gpos0, split_keys, split_gpos, parts,
+                                                         cta_counts);
+  HPCS_CUDA(cudaGetLastError());
+  shard_scan_kernel<<<1, 1024, 0, s>>>(cta_counts, grid, parts, cta_offsets, counts_out);
+  HPCS_CUDA(cudaGetLastError());
+  const size_t smem = size_t(2) * SHARD_SUB * parts * 4;
+  if (items)
+    shard_scatter_kernel<U, KIND, true><<<grid, SHARD_NT, smem, s>>>(keys, items, n, per_cta, gpos0, split_keys,
+                                                                     split_gpos, parts, cta_offsets, keys_out,
+                                                                     items_out);
+  else
+    shard_scatter_kernel<U, KIND, false><<<grid, SHARD_NT, smem, s>>>(keys, nullptr, n, per_cta, gpos0, split_keys,
+                                                                      split_gpos, parts, cta_offsets, keys_out,
+                                                                      nullptr);
+  HPCS_CUDA(cudaGetLastError());
+  return HPCS_OK;
+}
+
+template <class U, int KIND>
+int shard_partition_typed(hpcs_ctx* ctx, const void* keys, const uint32_t* items, int64_t n, int64_t gpos0,
+                          const void* split_keys, const int64_t* split_gpos, int parts, void* keys_out,
+                          uint32_t* items_out, int64_t* counts_out, cudaStream_t s) {
+  return enqueue_shard_partition<U, KIND>(ctx, static_cast<const U*>(keys), items, n, gpos0,
+                                          static_cast<const U*>(split_keys), split_gpos, parts,
+                                          static_cast<U*>(keys_out), items_out, counts_out, s);
+}
+
 }  // namespace
 }  // namespace hpcs
 
@@ -703,6 +752,36 @@ int hpcs_histogram_byte_components_dev(hpcs_ctx* ctx, int dtype, const void* a, 
     case HPCS_F64: return enqueue_histogram<uint64_t, KIND_FLOAT>(ctx, static_cast<const uint64_t*>(a), n, counts, s);
     default: return fail(HPCS_ERR_UNSUPPORTED, "unknown dtype");
   }
+}
+
+int hpcs_shard_partition_dev(hpcs_ctx* ctx, int dtype, const void* keys, const uint32_t* items, int64_t n,
+                             int64_t gpos0, const void* split_keys, const int64_t* split_gpos, int parts,
+                             void* keys_out, uint32_t* items_out, int64_t* counts_out, void* stream) {
+  int rc = check_common(ctx, keys, n);
+  if (rc != HPCS_OK) return rc;
+  if (!keys_out || !counts_out) return fail(HPCS_ERR_NULL, "keys_out or counts_out is NULL");
+  if ((items == nullptr) != (items_out == nullptr)) return fail(HPCS_ERR_NULL, "items and items_out must both be set");
+  if (parts < 1 || parts > HPCS_MAX_PARTS) return fail(HPCS_ERR_RANGE, "parts must be in [1, HPCS_MAX_PARTS]");
+  if (parts > 1 && (!split_keys || !split_gpos)) return fail(HPCS_ERR_NULL, "splitters are NULL");
+  if (gpos0 < 0) return fail(HPCS_ERR_RANGE, "gpos0 is negative");
+  if (keys_out == keys) return fail(HPCS_ERR_RANGE, "keys_out must not overlap keys");
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = pick_stream(ctx, stream);
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+#define HPCS_SHARD_CASE(DT, U, KIND) \
+  case DT:                          \
+    return shard_partition_typed<U, KIND>(ctx, keys, items, n, gpos0, split_keys, split_gpos, parts, keys_out, \
+                                          items_out, counts_out, s);
+  switch (dtype) {
+    HPCS_SHARD_CASE(HPCS_U32, uint32_t, KIND_UNSIGNED)
+    HPCS_SHARD_CASE(HPCS_I32, uint32_t, KIND_SIGNED)
+    HPCS_SHARD_CASE(HPCS_F32, uint32_t, KIND_FLOAT)
+    HPCS_SHARD_CASE(HPCS_U64, uint64_t, KIND_UNSIGNED)
+    HPCS_SHARD_CASE(HPCS_I64, uint64_t, KIND_SIGNED)
+    HPCS_SHARD_CASE(HPCS_F64, uint64_t, KIND_FLOAT)
+    default: return fail(HPCS_ERR_UNSUPPORTED, "unknown dtype");
+  }
+#undef HPCS_SHARD_CASE
 }
 
 }  // extern "C"

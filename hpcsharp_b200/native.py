@@ -79,7 +79,7 @@ class HpcsConfig(C.Structure):
 
 
 PASS_SCHEMES = {"auto": 0, "lookback": 1, "chunked": 2}
-KCLASS = {"histogram": 0, "onesweep": 1, "finalize": 2, "topk": 3, "segmented": 4}
+KCLASS = {"histogram": 0, "onesweep": 1, "finalize": 2, "topk": 3, "segmented": 4, "shard": 5}
 
 
 class HpcsSegment(C.Structure):
@@ -156,6 +156,7 @@ def _declare(lib) -> None:
         getattr(lib, f"hpcs_topk_largest_{t}").argtypes = [P, P, I64, I64, P]
         getattr(lib, f"hpcs_topk_largest_{t}_dev").argtypes = [P, P, I64, I64, P, P]
     lib.hpcs_histogram_byte_components_dev.argtypes = [P, I32, P, I64, P, P]
+    lib.hpcs_shard_partition_dev.argtypes = [P, I32, P, P, I64, I64, P, P, I32, P, P, P, P]
     for t in COUNT_NP_OF:
         getattr(lib, f"hpcs_sort_{t}").argtypes = [P, P, I64]
         getattr(lib, f"hpcs_sort_{t}_dev").argtypes = [P, P, I64, P]
@@ -390,6 +391,16 @@ class Context:
                                                           _ptr(counts), stream))
 
 
+    def shard_partition_dev(self, keys, items, gpos0: int, split_keys, split_gpos, parts: int, keys_out,
+                            items_out, counts_out, dtype: str | None = None, stream: int | None = None) -> None:
+        """Stable partition of a shard into `parts` parts by (key, global position) splitters
+        (hpcs_shard_partition_dev); counts_out receives the parts' sizes (int64)."""
+        name = dtype or _torch_dtype_name(keys)
+        check(self.lib.hpcs_shard_partition_dev(self.handle, DTYPES[name], _ptr(keys), _ptr(items), keys.numel(),
+                                                gpos0, _ptr(split_keys), _ptr(split_gpos), parts, _ptr(keys_out),
+                                                _ptr(items_out), _ptr(counts_out), stream))
+
+
 def make_segments(segments):
     arr = (HpcsSegment * len(segments))()
     for i, (t, dt) in enumerate(segments):
@@ -426,6 +437,16 @@ class SegPlan:
             self.close()
         except Exception:
             pass
+
+
+def torch_stream(device=None) -> int:
+    """The stream argument of the *_dev calls that runs them on torch's current stream of
+    `device`.  Torch's default stream has the handle 0, which the C ABI reads as the context's
+    own stream, so it is passed as cudaStreamLegacy (1)."""
+    import torch
+
+    h = torch.cuda.current_stream(device).cuda_stream
+    return h if h else 1
 
 
 def _torch_dtype_name(t) -> str:

@@ -20,8 +20,10 @@
  *     the GPU, sort, copy back into the same array and return.  The result is the
  *     reference's in-place result (the caller's array sorted, RadixSortLsdParallel.cs:227-231).
  *   - *_dev functions take device pointers and a cudaStream_t (passed as void*, NULL = the
- *     context's own stream); they are asynchronous on that stream.  Device-side failures
- *     (bounded waits that ran out) are reported by the next hpcs_ctx_synchronize().
+ *     context's own stream, which does not synchronise with the legacy default stream; pass
+ *     cudaStreamLegacy, (void*)1, to run on that one); they are asynchronous on that stream.
+ *     Device-side failures (bounded waits that ran out) are reported by the next
+ *     hpcs_ctx_synchronize().
  *   - A context is used by one host thread at a time.  Its scratch memory is reused
  *     across calls in stream order.
  *   - Sorting is stable and ascending.  Signed keys order by value; float keys order by
@@ -109,6 +111,7 @@ typedef enum hpcs_kernel_class {
   HPCS_K_FINALIZE = 2,  /* copy-back / error fold */
   HPCS_K_TOPK = 3,      /* radix select kernels */
   HPCS_K_SEGMENTED = 4, /* batched segmented sort kernels */
+  HPCS_K_SHARD = 5,     /* sharded sort: partition of a shard (count, scan, scatter) */
   HPCS_K_CLASSES = 8
 } hpcs_kernel_class;
 
@@ -364,6 +367,28 @@ int hpcs_server_destroy(hpcs_server* server);
  *     from several streams or host threads at once -- race and corrupt each other. */
 #define HPCS_NOALLOC_MAX_KEYS ((int64_t)1048576) /* 2^20 keys */
 int hpcs_sort_u32_dev_noalloc(uint32_t* keys, int64_t n, void* stream);
+
+/* ---- sort of one array spread over ranks: the per-rank partition step -----------------
+ * No single reference call: HPCsharp sorts one array per process, splitting it across host
+ * threads (SortRadixPar, RadixSortLsdParallel.cs:49-232).  The sharded sort (one process per
+ * GPU) keeps its result -- the concatenation of the ranks' outputs is the stable sort of the
+ * concatenation of their inputs -- by partitioning each rank's shard with parts-1 splitters,
+ * exchanging the parts (NCCL all-to-all) and sorting what each rank received with the plain
+ * sort (hpcs_sort_*_dev / hpcs_sort_pairs_*_dev).
+ *
+ * Element i of the shard has global position gpos0 + i.  It goes to part b = the number of
+ * splitters (split_keys[j], split_gpos[j]) at or below (keys[i], gpos0 + i), comparing keys
+ * in the sort's order (signed and float transforms) and then positions; so equal keys may be
+ * split between parts.  The splitters must ascend in that order.  The partition is stable:
+ * part b is keys_out[off_b .. off_b + counts_out[b]), off_b = counts of the parts below b, in
+ * shard order.  All pointers are device pointers; items / items_out are both NULL (keys only)
+ * or both set; keys_out must not overlap keys; counts_out receives parts int64 counts.
+ *   - parts outside [1, HPCS_MAX_PARTS], n outside [0, HPCS_MAX_KEYS] or gpos0 < 0 ->
+ *     HPCS_ERR_RANGE; a NULL array (splitters only when parts > 1) -> HPCS_ERR_NULL. */
+#define HPCS_MAX_PARTS 64
+int hpcs_shard_partition_dev(hpcs_ctx* ctx, int dtype, const void* keys, const uint32_t* items, int64_t n,
+                             int64_t gpos0, const void* split_keys, const int64_t* split_gpos, int parts,
+                             void* keys_out, uint32_t* items_out, int64_t* counts_out, void* stream);
 
 #ifdef __cplusplus
 }

@@ -28,7 +28,7 @@ def test_plain_sort_at_scale(ctx, dt, n, gen):
     a = gen(n)
     t = to_dev(a)
     before = checksum_dev(t)
-    ctx.sort_dev(t, dtype=dt, stream=torch.cuda.current_stream().cuda_stream)
+    ctx.sort_dev(t, dtype=dt, stream=native.torch_stream())
     torch.cuda.synchronize()
     ctx.synchronize()
     assert is_sorted_dev(t, dt)
@@ -51,7 +51,7 @@ def test_pairs_at_scale(ctx, dt, n, gen):
     keys = to_dev(a)
     orig = keys.clone()
     items = torch.arange(n, dtype=torch.int32, device="cuda")
-    ctx.sort_pairs_dev(keys, items, dtype=dt, stream=torch.cuda.current_stream().cuda_stream)
+    ctx.sort_pairs_dev(keys, items, dtype=dt, stream=native.torch_stream())
     torch.cuda.synchronize()
     ctx.synchronize()
     assert is_sorted_dev(keys, dt)
@@ -80,7 +80,7 @@ def test_sort_beyond_2_to_30_keys(ctx):
     t = to_dev(a)
     del a
     before = checksum_dev(t)
-    ctx.sort_dev(t, dtype="u32", stream=torch.cuda.current_stream().cuda_stream)
+    ctx.sort_dev(t, dtype="u32", stream=native.torch_stream())
     torch.cuda.synchronize()
     ctx.synchronize()
     assert is_sorted_dev(t, "u32")
@@ -90,7 +90,7 @@ def test_sort_beyond_2_to_30_keys(ctx):
     orig = keys.clone()
     del t
     items = torch.arange(n, dtype=torch.int32, device="cuda")
-    ctx.sort_pairs_dev(keys, items, dtype="u32", stream=torch.cuda.current_stream().cuda_stream)
+    ctx.sort_pairs_dev(keys, items, dtype="u32", stream=native.torch_stream())
     torch.cuda.synchronize()
     ctx.synchronize()
     assert is_sorted_dev(keys, "u32")

@@ -42,7 +42,7 @@ def test_single_dtype_batch(ctx, orc, dt):
     host = make_batch(11, dtypes=[dt])
     devs = [to_dev(a) if a.size else torch.empty(0, device="cuda") for a, _ in host]
     ctx.sort_segmented_dev([(t, d) for t, (_, d) in zip(devs, host)],
-                           stream=torch.cuda.current_stream().cuda_stream)
+                           stream=native.torch_stream())
     torch.cuda.synchronize()
     ctx.synchronize()
     check(host, devs, orc)
@@ -56,7 +56,7 @@ def test_mixed_batch_many_small(ctx, orc):
     host = make_batch(7, lengths=lengths)
     devs = [to_dev(a) for a, _ in host]
     ctx.sort_segmented_dev([(t, d) for t, (_, d) in zip(devs, host)],
-                           stream=torch.cuda.current_stream().cuda_stream)
+                           stream=native.torch_stream())
     torch.cuda.synchronize()
     ctx.synchronize()
     check(host, devs, orc)
@@ -69,7 +69,7 @@ def test_plan_graph_replays(ctx, orc):
     devs = [to_dev(a) if a.size else torch.empty(0, device="cuda") for a, _ in host]
     plan = ctx.segplan([(t, d) for t, (_, d) in zip(devs, host)])
     try:
-        s = torch.cuda.current_stream().cuda_stream
+        s = native.torch_stream()
         plan.execute(s)
         torch.cuda.synchronize()
         ctx.synchronize()
@@ -95,7 +95,7 @@ def test_segmented_equals_plain_sort(ctx):
     host = make_batch(33, lengths=[5000, 9000, 123_457, 1_000_003])
     a_dev = [to_dev(a) for a, _ in host]
     b_dev = [to_dev(a) for a, _ in host]
-    s = torch.cuda.current_stream().cuda_stream
+    s = native.torch_stream()
     ctx.sort_segmented_dev([(t, d) for t, (_, d) in zip(a_dev, host)], stream=s)
     for t, (_, d) in zip(b_dev, host):
         ctx.sort_dev(t, dtype=d, stream=s)
@@ -149,7 +149,7 @@ def test_every_variant_matches_oracle(orc, variant):
         host = make_batch(30 + variant, lengths=lengths)
         devs = [to_dev(a) if a.size else torch.empty(0, device="cuda") for a, _ in host]
         segs = [(t, d) for t, (_, d) in zip(devs, host)]
-        c.sort_segmented_dev(segs, stream=torch.cuda.current_stream().cuda_stream)
+        c.sort_segmented_dev(segs, stream=native.torch_stream())
         torch.cuda.synchronize()
         c.synchronize()
         check(host, devs, orc)

@@ -138,7 +138,7 @@ def test_device_sort_parity(ctx, orc, dt, offset):
     a = datagen.by_name(dt, 777_777, seed=21)
     want = oracle_sorted(orc, a)
     t = to_dev(a, offset)
-    ctx.sort_dev(t, dtype=dt, stream=torch.cuda.current_stream().cuda_stream)
+    ctx.sort_dev(t, dtype=dt, stream=native.torch_stream())
     torch.cuda.synchronize()
     ctx.synchronize()
     assert_same_bits(from_dev(t, a.dtype), want)
@@ -290,7 +290,7 @@ def test_counting_sort_device_unaligned(ctx):
     big = torch.zeros(a.size + 3, dtype=torch.int16, device="cuda")
     big[3:].copy_(t)
     lib = native.load()
-    native.check(lib.hpcs_sort_u16_dev(ctx.handle, big.data_ptr() + 6, a.size, torch.cuda.current_stream().cuda_stream))
+    native.check(lib.hpcs_sort_u16_dev(ctx.handle, big.data_ptr() + 6, a.size, native.torch_stream()))
     torch.cuda.synchronize()
     ctx.synchronize()
     assert np.array_equal(big[3:].cpu().numpy().view(np.uint16), np.sort(a))

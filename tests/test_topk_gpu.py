@@ -83,7 +83,7 @@ def test_topk_largest_device(ctx, orc):
     a = datagen.f32_normal_special(n, seed=9)
     t = to_dev(a)
     out = torch.empty(k, dtype=torch.int32, device="cuda")
-    ctx.topk_largest_dev(t, k, out, dtype="f32", stream=torch.cuda.current_stream().cuda_stream)
+    ctx.topk_largest_dev(t, k, out, dtype="f32", stream=native.torch_stream())
     torch.cuda.synchronize()
     ctx.synchronize()
     np.testing.assert_array_equal(bits(from_dev(out, np.float32)), sorted_bits(orc, a)[n - k:])
@@ -95,7 +95,7 @@ def test_select_topk_device_in_place(ctx, orc):
     n, k = 1_000_003, 333_333
     a = datagen.u64_uniform(n, seed=4)
     t = to_dev(a)
-    ctx.select_topk_dev(t, k, dtype="u64", stream=torch.cuda.current_stream().cuda_stream)
+    ctx.select_topk_dev(t, k, dtype="u64", stream=native.torch_stream())
     torch.cuda.synchronize()
     ctx.synchronize()
     got = from_dev(t, np.uint64)
