@@ -114,10 +114,13 @@ CASES = {  # name: (dtype, shard sizes)
 }
 
 
-def _global(name: str):
+def _global(name: str, world: int):
+    """(dtype, shard sizes of `world` ranks, global array); with fewer ranks than the case
+    lists, the last rank takes the remaining shards."""
     dt, sizes = CASES[name]
     rng = np.random.default_rng(len(name) * 1009 + sizes[0])
-    return dt, sizes, _keys(dt, sum(sizes), rng, dup=name.endswith("_dup"))
+    a = _keys(dt, sum(sizes), rng, dup=name.endswith("_dup"))
+    return dt, sizes[:world - 1] + [sum(sizes[world - 1:])], a
 
 
 def _rank(rank, world, port, backend, names, q):
@@ -135,7 +138,7 @@ def _rank(rank, world, port, backend, names, q):
     try:
         out = {}
         for name in names:
-            dt, sizes, a = _global(name)
+            dt, sizes, a = _global(name, world)
             lo = sum(sizes[:rank])
             shard = a[lo: lo + sizes[rank]]
             keys = torch.from_numpy(shard.view(VIEW[shard.dtype.itemsize]).copy()).cuda()
@@ -162,7 +165,7 @@ def _run(world, backend, names):
         p.start()
     res = collect(q, procs, limit_s=LIMIT_S)
     for name in names:
-        dt, sizes, a = _global(name)
+        dt, sizes, a = _global(name, world)
         perm = np.argsort(oracle.order_key(a), kind="stable")
         want = a[perm].view(VIEW[a.dtype.itemsize])
         for balance in (True, False):
