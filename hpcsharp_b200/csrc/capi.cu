@@ -413,9 +413,48 @@ int topk_largest_host(hpcs_ctx* ctx, const T* in, int64_t n, int64_t k, T* out) 
   return check_device_errors(ctx);
 }
 
-// Count, scan and scatter of one shard into `parts` parts (shard.cuh).  Three CTAs per SM
-// (the scatter kernel's 80 registers x 256 threads allow three), each a contiguous range of
-// whole tiles; both passes use the same ranges.
+// Count, scan and scatter of one shard into `parts` parts (shard.cuh), the kernels built
+// for LOG = ceil(log2(parts)).  shard_ctas_per_sm CTAs per SM (the scatter kernel's register
+// budget), each a contiguous range of whole tiles; both passes use the same ranges.
+template <class U, int KIND, int LOG>
+int launch_shard_partition(hpcs_ctx* ctx, const U* keys, const uint32_t* items, int64_t n, int64_t gpos0,
+                           const U* split_keys, const int64_t* split_gpos, int parts, U* keys_out,
+                           uint32_t* items_out, int64_t* counts_out, cudaStream_t s) {
+  const int64_t tiles = (n + SHARD_TILE - 1) / SHARD_TILE;
+  const int64_t cap = int64_t(ctx->sms) * (items ? shard_ctas_per_sm<U, true>() : shard_ctas_per_sm<U, false>());
+  const int grid = int(tiles < cap ? tiles : cap);
+  const int64_t per_cta = (tiles + grid - 1) / grid * SHARD_TILE;
+  int rc;
+  if ((rc = ensure(ctx, ctx->aux0, size_t(grid) * parts * 4)) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->aux1, size_t(grid) * parts * 8)) != HPCS_OK) return rc;
+  uint32_t* cta_counts = static_cast<uint32_t*>(ctx->aux0.ptr);
+  int64_t* cta_offsets = static_cast<int64_t*>(ctx->aux1.ptr);
+  static int attr_set[64] = {0};  // per instance: the scatter kernels' shared memory limit
+  if (!attr_set[ctx->device & 63]) {
+    HPCS_CUDA(cudaFuncSetAttribute(shard_scatter_kernel<U, KIND, true, LOG>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(shard_scatter_smem<U, true>(SHARD_MAX_PARTS))));
+    HPCS_CUDA(cudaFuncSetAttribute(shard_scatter_kernel<U, KIND, false, LOG>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(shard_scatter_smem<U, false>(SHARD_MAX_PARTS))));
+    attr_set[ctx->device & 63] = 1;
+  }
+  KernelTimer kt(ctx, s, HPCS_K_SHARD);
+  shard_count_kernel<U, KIND, LOG><<<grid, SHARD_COUNT_NT, 0, s>>>(keys, n, per_cta, gpos0, split_keys, split_gpos,
+                                                                   parts, cta_counts);
+  HPCS_CUDA(cudaGetLastError());
+  shard_scan_kernel<<<1, 1024, 0, s>>>(cta_counts, grid, parts, cta_offsets, counts_out);
+  HPCS_CUDA(cudaGetLastError());
+  if (items)
+    shard_scatter_kernel<U, KIND, true, LOG><<<grid, SHARD_NT, shard_scatter_smem<U, true>(parts), s>>>(
+        keys, items, n, per_cta, gpos0, split_keys, split_gpos, parts, cta_offsets, keys_out, items_out);
+  else
+    shard_scatter_kernel<U, KIND, false, LOG><<<grid, SHARD_NT, shard_scatter_smem<U, false>(parts), s>>>(
+        keys, nullptr, n, per_cta, gpos0, split_keys, split_gpos, parts, cta_offsets, keys_out, nullptr);
+  HPCS_CUDA(cudaGetLastError());
+  return HPCS_OK;
+}
+
 template <class U, int KIND>
 int enqueue_shard_partition(hpcs_ctx* ctx, const U* keys, const uint32_t* items, int64_t n, int64_t gpos0,
                             const U* split_keys, const int64_t* split_gpos, int parts, U* keys_out,
@@ -424,32 +463,23 @@ int enqueue_shard_partition(hpcs_ctx* ctx, const U* keys, const uint32_t* items,
     HPCS_CUDA(cudaMemsetAsync(counts_out, 0, size_t(parts) * 8, s));
     return HPCS_OK;
   }
-  const int64_t tiles = (n + SHARD_TILE - 1) / SHARD_TILE;
-  const int64_t cap = int64_t(ctx->sms) * 3;
-  const int grid = int(tiles < cap ? tiles : cap);
-  const int64_t per_cta = (tiles + grid - 1) / grid * SHARD_TILE;
-  int rc;
-  if ((rc = ensure(ctx, ctx->aux0, size_t(grid) * parts * 4)) != HPCS_OK) return rc;
-  if ((rc = ensure(ctx, ctx->aux1, size_t(grid) * parts * 8)) != HPCS_OK) return rc;
-  uint32_t* cta_counts = static_cast<uint32_t*>(ctx->aux0.ptr);
-  int64_t* cta_offsets = static_cast<int64_t*>(ctx->aux1.ptr);
-  KernelTimer kt(ctx, s, HPCS_K_SHARD);
-  shard_count_kernel<U, KIND><<<grid, SHARD_NT, 0, s>>>(keys, n, per_cta, gpos0, split_keys, split_gpos, parts,
-                                                         cta_counts);
-  HPCS_CUDA(cudaGetLastError());
-  shard_scan_kernel<<<1, 1024, 0, s>>>(cta_counts, grid, parts, cta_offsets, counts_out);
-  HPCS_CUDA(cudaGetLastError());
-  const size_t smem = size_t(2) * SHARD_SUB * parts * 4;
-  if (items)
-    shard_scatter_kernel<U, KIND, true><<<grid, SHARD_NT, smem, s>>>(keys, items, n, per_cta, gpos0, split_keys,
-                                                                     split_gpos, parts, cta_offsets, keys_out,
-                                                                     items_out);
-  else
-    shard_scatter_kernel<U, KIND, false><<<grid, SHARD_NT, smem, s>>>(keys, nullptr, n, per_cta, gpos0, split_keys,
-                                                                      split_gpos, parts, cta_offsets, keys_out,
-                                                                      nullptr);
-  HPCS_CUDA(cudaGetLastError());
-  return HPCS_OK;
+  int log = 0;
+  while ((1 << log) < parts) log++;
+#define HPCS_SHARD_LOG(L)                                                                                      \
+  case L:                                                                                                      \
+    return launch_shard_partition<U, KIND, L>(ctx, keys, items, n, gpos0, split_keys, split_gpos, parts, keys_out, \
+                                              items_out, counts_out, s);
+  switch (log) {
+    HPCS_SHARD_LOG(0)
+    HPCS_SHARD_LOG(1)
+    HPCS_SHARD_LOG(2)
+    HPCS_SHARD_LOG(3)
+    HPCS_SHARD_LOG(4)
+    HPCS_SHARD_LOG(5)
+    HPCS_SHARD_LOG(6)
+    default: return fail(HPCS_ERR_RANGE, "parts must be in [1, HPCS_MAX_PARTS]");
+  }
+#undef HPCS_SHARD_LOG
 }
 
 template <class U, int KIND>
