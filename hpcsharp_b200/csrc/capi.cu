@@ -582,8 +582,9 @@ int hpcs_ctx_destroy(hpcs_ctx* ctx) {
   DeviceGuard g(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->last_stream && ctx->last_stream != ctx->stream) cudaStreamSynchronize(ctx->last_stream);
-  DevBuf* bufs[] = {&ctx->keys_a, &ctx->keys_b, &ctx->vals_a, &ctx->vals_b, &ctx->status0, &ctx->status1,
-                    &ctx->plan,   &ctx->counts, &ctx->err_accum, &ctx->aux0, &ctx->aux1, &ctx->aux2};
+  DevBuf* bufs[] = {&ctx->keys_a, &ctx->keys_b,  &ctx->vals_a,    &ctx->vals_b, &ctx->status0,
+                    &ctx->status1, &ctx->status2, &ctx->plan, &ctx->counts, &ctx->err_accum,
+                    &ctx->aux0,   &ctx->aux1,    &ctx->aux2};
   for (DevBuf* b : bufs)
     if (b->ptr && !b->borrowed) cudaFree(b->ptr);
   for (auto& t : ctx->timed) {

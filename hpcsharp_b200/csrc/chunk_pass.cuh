@@ -80,6 +80,7 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
 
   const SortPlan* plan = args.plan;
   const int pass = args.pass;
+  if (args.choose_lookback && plan->use_lookback) return;  // the look-back passes were chosen
   const int sel = plan->src_sel[pass];
   if (sel < 0) return;  // every key has the same digit here: the pass is the identity
   const int shift = 8 * pass;

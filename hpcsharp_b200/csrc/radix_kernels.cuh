@@ -66,6 +66,7 @@ struct SortPlan {
   int32_t skewed[MAX_PASSES];             // 1 when that value holds more than 1/32 of the keys
   int32_t heavy2[MAX_PASSES];             // the second most frequent value
   int32_t grouped[MAX_PASSES];            // 1 when the two hold more than 3/4 of the keys
+  int32_t use_lookback;                   // device-chosen scheme (SortArgs::choose_lookback)
 };
 
 struct SortArgs {
@@ -94,6 +95,10 @@ struct SortArgs {
   int chunks;
   uint32_t chunk_keys;
   uint32_t chunk_magic;   // ceil(2^32 / chunk_keys): range of position p = umulhi(p, magic) (-1)
+  // 1: K1 chooses the scheme from the digit counts (plan->use_lookback); both the chunked and
+  // the look-back passes are launched and the ones not chosen return at once.  The look-back
+  // status buffers (status[]) are then separate from the chunked tables.
+  int choose_lookback;
 };
 constexpr int TRACE_WORDS = 7;
 
@@ -283,6 +288,15 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
       }
     }
     plan->final_sel = sel;
+    // Device-chosen passes: look-back when an executed digit has one value above 1/8 of the
+    // keys but no two values holding 3/4 of them (several frequent values, as in the sign and
+    // exponent byte of normally distributed floats): counting those for the next pass's
+    // per-range tables costs the chunked passes more than the look-back.  Otherwise chunked.
+    int lb = 0;
+    if (args.choose_lookback)
+      for (int d = 0; d < P; d++)
+        if (plan->exec_idx[d] >= 0 && int64_t(s_heavy[d] >> 8) > n / 8 && !plan->grouped[d]) lb = 1;
+    plan->use_lookback = lb;
     __threadfence();
   }
 }
@@ -431,6 +445,7 @@ __global__ void __launch_bounds__(NT, MINB) onesweep_pass_kernel(SortArgs args) 
 
   const SortPlan* plan = args.plan;
   const int pass = args.pass;
+  if (args.choose_lookback && !plan->use_lookback) return;  // the chunked passes were chosen
   const int sel = plan->src_sel[pass];
   if (sel < 0) return;  // every key has the same digit here: the pass is the identity (uniform)
   const int shift = 8 * pass;

@@ -59,6 +59,7 @@ struct hpcs_ctx {
   std::vector<cudaEvent_t> event_pool;
   // scratch
   hpcs::DevBuf keys_a, keys_b, vals_a, vals_b, status0, status1, plan, counts, err_accum;
+  hpcs::DevBuf status2;  // second look-back buffer when the device chooses the scheme
   hpcs::DevBuf aux0, aux1, aux2;
   // batched segmented sort: variant per (key width, length class), and the helper streams
   // and events that run the launches of different variants concurrently
@@ -335,9 +336,14 @@ int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t
     return fail(HPCS_ERR_RANGE, "look-back passes take at most 2^30 - 1 keys (30-bit prefixes)");
   const bool lookback = ctx->cfg.pass_scheme == HPCS_PASSES_LOOKBACK ||
                         (ctx->cfg.pass_scheme != HPCS_PASSES_CHUNKED && n < ChunkMinKeys<U, V>::value);
+  // 4-byte float keys without items, AUTO scheme, large sorts: K1 picks the scheme from the
+  // digit counts (normally distributed floats sort faster with the look-back passes, floats
+  // with a dominant exponent with the chunked ones).  Not on borrowed (serving) scratch.
+  const bool choose = !lookback && ctx->cfg.pass_scheme == HPCS_PASSES_AUTO && KIND == KIND_FLOAT &&
+                      sizeof(U) == 4 && !PAIRS && n <= MAX_KEYS_LOOKBACK && !ctx->status1.borrowed;
   const bool ordered = ctx->rank_mode == RANK_ORDERED_ATOMIC;
   const int64_t unit = ordered ? int64_t(CA::NT) * CA::KPT * CA::CL : int64_t(CP::NT) * CP::KPT * CP::CL;
-  const int64_t num_tiles = lookback ? (n + unit - 1) / unit : 0;  // look-back units
+  const int64_t num_tiles = lookback || choose ? (n + unit - 1) / unit : 0;  // look-back units
   ChunkGeometry geo{0, 0, 0};
   if (!lookback) {
     using SA = ChunkShape<U, V, RANK_ORDERED_ATOMIC>;
@@ -368,6 +374,9 @@ int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t
   const size_t status_bytes = lookback ? size_t(num_tiles) * RADIX * 4 : size_t(geo.chunks) * (P + 3) * RADIX * 4;
   if ((rc = ensure(ctx, ctx->status0, status_bytes)) != HPCS_OK) return rc;
   if (lookback && (rc = ensure(ctx, ctx->status1, status_bytes)) != HPCS_OK) return rc;
+  const size_t lb_bytes = size_t(num_tiles) * RADIX * 4;  // one look-back buffer (choose)
+  if (choose && (rc = ensure(ctx, ctx->status1, lb_bytes)) != HPCS_OK) return rc;
+  if (choose && (rc = ensure(ctx, ctx->status2, lb_bytes)) != HPCS_OK) return rc;
   if ((rc = ensure(ctx, ctx->plan, sizeof(SortPlan))) != HPCS_OK) return rc;
 
   SortArgs args{};
@@ -394,6 +403,14 @@ int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t
     args.chunk_keys = geo.chunk_keys;
     args.chunk_magic = geo.magic;
   }
+  if (choose) {
+    // the look-back passes' buffers are status1 and status2; K1 (chunked mode) does not
+    // zero the first one, so it is cleared here
+    args.choose_lookback = 1;
+    args.status[0] = static_cast<uint32_t*>(ctx->status1.ptr);
+    args.status[1] = static_cast<uint32_t*>(ctx->status2.ptr);
+    HPCS_CUDA(cudaMemsetAsync(args.status[0], 0, lb_bytes, s));
+  }
 
   HPCS_CUDA(cudaMemsetAsync(args.plan, 0, sizeof(SortPlan), s));
 
@@ -402,11 +419,11 @@ int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t
     KernelTimer kt(ctx, s, HPCS_K_HISTOGRAM);
     if ((rc = launch_histogram<U, KIND>(ctx, a, n, &args.plan->hist[0][0], args, 1, s)) != HPCS_OK) return rc;
   }
-  // K3: one launch per digit
+  // K3: one launch per digit (with `choose`, both kinds; the ones K1 did not choose return)
   if (!lookback)
     rc = ordered ? launch_chunk_passes<U, KIND, V, RANK_ORDERED_ATOMIC>(ctx, args, s)
                  : launch_chunk_passes<U, KIND, V, RANK_PEER_MASK>(ctx, args, s);
-  else
+  if (rc == HPCS_OK && (lookback || choose))
     rc = ordered ? launch_onesweep_passes<U, KIND, V, RANK_ORDERED_ATOMIC>(ctx, args, s)
                  : launch_onesweep_passes<U, KIND, V, RANK_PEER_MASK>(ctx, args, s);
   if (rc != HPCS_OK) return rc;

@@ -97,3 +97,40 @@ def test_scheme_skewed_digits(sctx, orc, dist):
     sctx.sort_pairs(kg, ig)
     assert np.array_equal(kg.view(np.uint8), ko.view(np.uint8))
     assert np.array_equal(ig, io)
+
+
+@pytest.mark.parametrize("dist", ["normal_specials", "uniform01", "bits"])
+def test_auto_scheme_float_keys_choose_on_device(orc, dist):
+    """4-byte float keys past the chunked threshold under the automatic scheme: the histogram
+    kernel picks look-back passes (normal keys: several frequent sign-and-exponent bytes) or
+    chunked passes (uniform(0,1): two bytes hold most keys; uniform bits: no frequent value),
+    and launches of the other kind return at once.  Every choice gives the oracle's bits."""
+    import torch
+
+    from tests.gpu_util import from_dev, to_dev
+
+    n = 52_000_003  # above the 48 Mi-key chunked threshold, ragged
+    rng = np.random.default_rng(11)
+    if dist == "normal_specials":
+        a = rng.standard_normal(n).astype(np.float32)
+        a[::97] = -0.0
+        a[::101] = 0.0
+        a[::103] = np.inf
+        a[::107] = -np.inf
+        a[::109] = np.float32("nan")
+        a[::113] = np.float32(1e-40)  # subnormal
+    elif dist == "uniform01":
+        a = rng.random(n, dtype=np.float32)
+    else:
+        a = rng.integers(0, 1 << 32, size=n, dtype=np.uint64).astype(np.uint32).view(np.float32)
+    c = native.Context(0)
+    try:
+        t = to_dev(a)
+        c.sort_dev(t, dtype="f32", stream=native.torch_stream())
+        torch.cuda.synchronize()
+        got = from_dev(t, np.float32)
+        c.synchronize()
+    finally:
+        c.close()
+    want = _oracle(orc, a)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
