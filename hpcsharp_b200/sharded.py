@@ -33,6 +33,7 @@ from __future__ import annotations
 import numpy as np
 
 SIGNED_VIEW = {4: "int32", 8: "int64"}
+MAX_PARTS = 64  # HPCS_MAX_PARTS of the C ABI: one part per rank
 
 
 def _torch():
@@ -155,6 +156,8 @@ def sort_sharded(keys, items=None, *, ops, group=None, samples: int = 1024, seed
     torch = _torch()
     comm = _Comm(group)
     world, rank = comm.world, comm.rank
+    if world > MAX_PARTS:
+        raise ValueError(f"sort_sharded takes at most {MAX_PARTS} ranks (one partition part per rank)")
     kb = _bits(keys)  # collectives, gathers and the ops see the keys' bytes as int32 / int64
     dev = kb.device
     n = kb.numel()
