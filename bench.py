@@ -314,13 +314,16 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     value = replicas.weak_scaling_gkeys(n, args.steps, world, total_ms)
     ms_per_step = total_ms / args.steps
 
-    # roofline of the dominant kernel (the chunked digit pass): algorithmic bytes per
-    # launch = one read + one write of the keys = 2 * n * w
-    os_launches, os_ms = prof["onesweep"]
+    # roofline of the dominant kernel, the digit pass of whichever scheme ran (chunked:
+    # profile class "onesweep", look-back: "lookback"; with float keys both kinds are launched
+    # and the kind not chosen returns at once): algorithmic bytes per launch = one read + one
+    # write of the keys = 2 * n * w
+    chunked_ran = prof["onesweep"][1] >= prof["lookback"][1]
+    os_launches, os_ms = prof["onesweep"] if chunked_ran else prof["lookback"]
     os_avg_ms = os_ms / max(1, os_launches)
     os_bytes = 2.0 * n * w
     achieved = os_bytes / (os_avg_ms / 1e3) / 1e9 if os_launches else None
-    roof = {"kernel": "chunk_pass", "bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
+    roof = {"kernel": "chunk_pass" if chunked_ran else "onesweep_pass (look-back)", "bound": "hbm", "achieved": round(achieved, 1) if achieved else None,
             "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
             "frac": round(achieved / hbm, 4) if achieved else None,
             "traffic": read_traffic(dtype), "algorithmic_bytes_per_launch": os_bytes,

@@ -278,7 +278,7 @@ int launch_onesweep_passes(hpcs_ctx* ctx, SortArgs args, cudaStream_t s) {
   cfg.gridDim = dim3(grid_clusters * C::CL, 1, 1);
   for (int p = 0; p < P; p++) {
     args.pass = p;
-    KernelTimer kt(ctx, s, HPCS_K_ONESWEEP);
+    KernelTimer kt(ctx, s, HPCS_K_LOOKBACK);
     HPCS_CUDA(cudaLaunchKernelEx(&cfg, k, args));
   }
   return HPCS_OK;

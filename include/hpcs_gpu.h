@@ -107,11 +107,13 @@ int hpcs_abi_version(void);
  * reference has commented-out Stopwatch blocks in its hot loops, RadixSortLsd.cs:146-153). */
 typedef enum hpcs_kernel_class {
   HPCS_K_HISTOGRAM = 0, /* fused all-digit histogram (+ plan) */
-  HPCS_K_ONESWEEP = 1,  /* one 8-bit digit pass */
+  HPCS_K_ONESWEEP = 1,  /* one 8-bit digit pass, chunked scheme */
   HPCS_K_FINALIZE = 2,  /* copy-back / error fold */
   HPCS_K_TOPK = 3,      /* radix select kernels */
   HPCS_K_SEGMENTED = 4, /* batched segmented sort kernels */
   HPCS_K_SHARD = 5,     /* sharded sort: partition of a shard (count, scan, scatter) */
+  HPCS_K_LOOKBACK = 6,  /* one 8-bit digit pass, decoupled look-back scheme (a launch whose
+                           scheme the histogram kernel did not choose returns at once) */
   HPCS_K_CLASSES = 8
 } hpcs_kernel_class;
 
