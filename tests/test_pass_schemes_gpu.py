@@ -74,7 +74,7 @@ def test_scheme_skipped_passes(sctx, orc, kind):
     assert np.array_equal(got, _oracle(orc, a))
 
 
-@pytest.mark.parametrize("dist", ["zipf", "few_values", "f32_normal"])
+@pytest.mark.parametrize("dist", ["zipf", "few_values", "f32_normal", "and3_u64", "and3_u32"])
 def test_scheme_skewed_digits(sctx, orc, dist):
     """Digits with frequent values: equal lanes' atomics are grouped (ranks by popcount)
     and the next pass's most frequent value is derived by subtraction; the bits and the
@@ -85,6 +85,13 @@ def test_scheme_skewed_digits(sctx, orc, dist):
     elif dist == "few_values":
         rng = np.random.default_rng(8)
         keys = rng.choice(np.array([7, 0xFF00FF, 1 << 40, 3], dtype=np.uint64), size=n, p=[0.6, 0.2, 0.15, 0.05])
+    elif dist == "and3_u64":  # 0 holds ~34% of every byte: one dominant value, not two
+        keys = datagen.u64_and3(n, seed=5)
+    elif dist == "and3_u32":
+        rng = np.random.default_rng(9)
+        keys = rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
+        for _ in range(2):
+            keys &= rng.integers(0, 1 << 32, n, dtype=np.uint64).astype(np.uint32)
     else:
         keys = datagen.f32_normal(n, seed=4)
     got = keys.copy()
