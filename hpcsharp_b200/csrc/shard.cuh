@@ -195,9 +195,9 @@ __global__ void __launch_bounds__(1024) shard_scan_kernel(const uint32_t* __rest
   for (int64_t i = tid; i < int64_t(grid) * parts; i += blockDim.x) cta_offsets[i] += s_base[i % parts];
 }
 
-// Pass 2: stable scatter of the CTA's range to its parts.  Per tile of SHARD_TILE keys (row r
-// of SHARD_NT keys holds keys t0 + r*SHARD_NT + tid, so sub-tile (r, warp) = r*NW + warp is in
-// key order):
+// Pass 2: stable scatter of the CTA's range to its parts.  Per tile of SHARD_TILE keys at
+// offset t of the range (row r of SHARD_NT keys holds keys t + r*SHARD_NT + tid, so sub-tile
+// (r, warp) = r*NW + warp is in key order):
 //   count:   each key's part; its rank among the same part's keys of its warp (ballots);
 //            the leader stores the (sub-tile, part) count;
 //   scan:    warp w scans parts w, w + NW, ...: the (sub-tile, part) base inside the part's
