@@ -53,12 +53,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="plain",
-                    choices=["plain", "batched", "served", "configs", "sharded"],
+                    choices=["plain", "batched", "served", "configs", "sharded", "kernels"],
                     help="plain: the 2^28-key sort (headline); batched: 65,536 mixed arrays; "
                          "served: Poisson sort/top-k requests swept to saturation; configs: every "
                          "plain-sort and pairs configuration, device-resident; sharded: one array of "
                          "--n keys per rank sorted across the ranks (partition, NCCL all-to-all, "
-                         "local sort, rebalance)")
+                         "local sort, rebalance); kernels: radix top-k, in-place SelectTopK and "
+                         "the 8/16-bit counting sorts, device-resident")
     ap.add_argument("--requests", type=int, default=120, help="served: requests per arrival rate")
     ap.add_argument("--loads", default="0.25,0.5,1,2,4,8,16",
                     help="served: offered loads, as multiples of the plain form's capacity")
@@ -694,6 +695,73 @@ def run_configs(args, rank: int, world: int, local_rank: int):
                       "steps": steps, "rows": rows}), flush=True)
 
 
+def run_kernels(args, rank: int, world: int, local_rank: int):
+    """The path's other entry points on device-resident keys, CUDA events on the context's
+    stream, input restored before each call outside the events, mean of up to 10 calls after 3
+    warm-ups: radix top-k (the k largest, out of place) of 2^28 u32 keys for k in {10, 1000,
+    100000}; SelectTopK in place (select + stable 3-way partition) of the same keys; the
+    counting sorts of 2^28 u8 and u16 keys.  Roofline bytes: top-k one read of the keys (its
+    minimum), SelectTopK the select's histogram read plus the partition's read and write,
+    counting sort one read (histogram) plus one write (fill)."""
+    import torch
+
+    from hpcsharp_b200 import datagen, native
+
+    if rank != 0:
+        return
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    hbm, peak_kind = peaks()
+    ctx = native.Context(dev)
+    s = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{dev}")
+    steps = max(1, min(args.steps, 10))
+    n = 1 << 28
+    rng = np.random.default_rng(5)
+    u32 = torch.from_numpy(datagen.u32_uniform(n, 1).view(np.int32)).to(f"cuda:{dev}")
+    u8 = torch.from_numpy(rng.integers(0, 256, n, dtype=np.uint8)).to(f"cuda:{dev}")
+    u16 = torch.from_numpy(rng.integers(0, 1 << 16, n, dtype=np.uint16).view(np.int16)).to(f"cuda:{dev}")
+    out = torch.empty(100_000, dtype=torch.int32, device=f"cuda:{dev}")
+    cases = []
+    for k in (10, 1000, 100_000):
+        cases.append((f"top-k largest, k={k}", "u32", u32, False,
+                      lambda t, k=k: ctx.topk_largest_dev(t, k, out[:k], dtype="u32", stream=ctx.stream), n * 4))
+    cases.append(("SelectTopK in place, k=n/2", "u32", u32, True,
+                  lambda t: ctx.select_topk_dev(t, n // 2, dtype="u32", stream=ctx.stream), 3 * n * 4))
+    cases.append(("counting sort", "u8", u8, True, lambda t: ctx.sort_dev(t, dtype="u8", stream=ctx.stream), 2 * n))
+    cases.append(("counting sort", "u16", u16, True, lambda t: ctx.sort_dev(t, dtype="u16", stream=ctx.stream),
+                  2 * n * 2))
+    rows = []
+    for name, dt, src, in_place, call, nbytes in cases:
+        buf = src.clone() if in_place else src
+        tot = 0.0
+        for i in range(3 + steps):
+            if in_place:
+                with torch.cuda.stream(s):
+                    buf.copy_(src)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s)
+            call(buf)
+            b.record(s)
+            ctx.synchronize()
+            if i >= 3:
+                tot += a.elapsed_time(b)
+        ms = tot / steps
+        gbs = nbytes / (ms / 1e3) / 1e9
+        rows.append({"op": name, "dtype": dt, "n": n, "ms": round(ms, 4), "gkeys_s": round(n / (ms / 1e3) / 1e9, 2),
+                     "roofline_bytes": nbytes, "achieved_gbs": round(gbs, 1), "roofline_frac": round(gbs / hbm, 4)})
+        if in_place and buf is not src:
+            del buf
+    srt = u8.clone()
+    ctx.sort_dev(srt, dtype="u8", stream=ctx.stream)
+    ctx.synchronize()
+    head = srt[:1 << 20].cpu().numpy()
+    if not np.all(head[1:] >= head[:-1]):
+        raise RuntimeError("counting sort result not in order")
+    ctx.close()
+    print(json.dumps({"metric": METRIC, "workload": "kernels", "unit": UNIT, "peak": hbm, "peak_kind": peak_kind,
+                      "steps": steps, "rows": rows}), flush=True)
+
+
 def run_sharded(args, rank: int, world: int, local_rank: int):
     """The sharded sort of one array of world x n keys (n per rank, weak scaling): every step
     partitions, exchanges (NCCL all-to-all), sorts and rebalances; CUDA events on the current
@@ -798,6 +866,9 @@ def main():
         return
     if args.workload == "sharded":
         run_sharded(args, rank, world, local_rank)
+        return
+    if args.workload == "kernels":
+        run_kernels(args, rank, world, local_rank)
         return
     run_ours(args, rank, world, local_rank)
 

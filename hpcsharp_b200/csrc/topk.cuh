@@ -11,12 +11,15 @@
 // compacted into a candidate buffer (about n/256 of them for spread keys) and the remaining
 // levels histogram only candidates that match the prefix chosen so far.  A one-block "pick"
 // kernel after each histogram advances the device-side SelectState, so nothing returns to the
-// host between levels.
+// host between levels.  The passes over all n keys read them with 16-byte loads, several in
+// flight per thread (visit_keys); compactions take one atomic per warp and vector row.
 //
 // Rearrangement: a stable three-way partition (keys < v, == v, > v around the selected key v)
 // in three kernels -- per-tile class counts, a one-block scan, a stable per-tile scatter.
 // The k largest ("top-k" of a serving request) are the keys > v, compacted, plus copies of v
 // up to k, then sorted ascending with the LSD sort so the output bytes are deterministic.
+// Keys above the level-0 bin are all > v: the level-0 compaction writes them to the output
+// at once, and the final gather scans only the candidates.  So top-k reads the n keys twice.
 #pragma once
 #include <cstdint>
 
@@ -31,13 +34,15 @@ struct SelectState {
   int64_t less;        // keys strictly below the prefix range
   int64_t eq;          // keys equal to the selected key (valid after the last level)
   int64_t cand_count;  // candidates compacted after level 0
-  unsigned long long gathered;  // keys > v written by topk_gather_kernel
+  unsigned long long gathered;  // keys > v written to the top-k output so far
+  int64_t n_total;     // keys selected among
   uint32_t hist[256];
 };
 
-static __global__ void select_init_kernel(SelectState* st, int64_t rank) {
+static __global__ void select_init_kernel(SelectState* st, int64_t rank, int64_t n) {
   const int tid = threadIdx.x;
   if (tid == 0) {
+    st->n_total = n;
     st->prefix = 0;
     st->mask = 0;
     st->rank = rank;
@@ -51,23 +56,150 @@ static __global__ void select_init_kernel(SelectState* st, int64_t rank) {
 
 constexpr int SEL_NT = 512;
 constexpr int SEL_COPIES = 32;
+constexpr int SEL_VPT = 4;  // 16-byte vectors in flight per thread
+constexpr int SEL_CTAS_PER_SM = 4;
+
+// Calls f(k, nv) for the keys of keys[0..n) in groups of E = 16 / sizeof(U): k holds E keys,
+// the first nv of them valid.  The 16-byte-aligned body goes as vectors, SEL_VPT per thread in
+// flight (vector j of a round at base + j*G + global thread id, G = grid threads); the
+// unaligned head (< E keys) and the ragged tail (< E keys) go to lanes 0 and 1 of the grid's
+// first warp.  Every lane of a warp makes the same calls (nv = 0 pads), so f may use warp
+// collectives.
+template <class U, class F>
+__device__ __forceinline__ void visit_keys(const U* __restrict__ keys, int64_t n, F&& f) {
+  constexpr int E = int(16 / sizeof(U));
+  union Vec {
+    uint4 v;
+    U k[E];
+  };
+  const uintptr_t addr = reinterpret_cast<uintptr_t>(keys);
+  int64_t head = int64_t(((16u - uint32_t(addr & 15u)) & 15u) / sizeof(U));
+  if (head > n) head = n;
+  const int64_t nvec = (n - head) / E;
+  const int64_t rest = head + nvec * E;  // first key of the tail
+  const uint4* vp = reinterpret_cast<const uint4*>(keys + head);
+  const int64_t G = int64_t(gridDim.x) * blockDim.x;
+  const int64_t gtid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (int64_t base = 0; base < nvec; base += G * SEL_VPT) {  // uniform over the grid
+    Vec v[SEL_VPT];
+#pragma unroll
+    for (int j = 0; j < SEL_VPT; j++) {
+      const int64_t idx = base + j * G + gtid;
+      v[j].v = idx < nvec ? __ldg(vp + idx) : make_uint4(0u, 0u, 0u, 0u);
+    }
+#pragma unroll
+    for (int j = 0; j < SEL_VPT; j++) f(v[j].k, base + j * G + gtid < nvec ? E : 0);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    Vec v;
+    v.v = make_uint4(0u, 0u, 0u, 0u);
+    int nv = 0;
+    if (lane == 0) {
+      nv = int(head);
+      for (int e = 0; e < nv; e++) v.k[e] = keys[e];
+    } else if (lane == 1) {
+      nv = int(n - rest);
+      for (int e = 0; e < nv; e++) v.k[e] = keys[rest + e];
+    }
+    f(v.k, nv);
+  }
+}
+
+// Appends the keys k[e] whose bit e of `take` is set to dst at a position drawn from *counter
+// (one atomic per warp); positions at or beyond `cap` are not written.  All lanes call it.
+template <class U, int E>
+__device__ __forceinline__ void warp_append(const U* k, uint32_t take, U* __restrict__ dst,
+                                            unsigned long long* counter, int64_t cap) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t c = __popc(take);
+  uint32_t incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  if (total == 0u) return;  // uniform over the warp
+  unsigned long long base = 0;
+  if (lane == 31) base = atomicAdd(counter, (unsigned long long)total);
+  base = __shfl_sync(0xFFFFFFFFu, base, 31);
+  unsigned long long pos = base + incl - c;
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    if ((take >> e) & 1u) {
+      if (int64_t(pos) < cap) dst[pos] = k[e];
+      pos++;
+    }
+  }
+}
+
+// Per-warp staging of appended keys in shared memory: a warp scan places each lane's keys in
+// the warp's CAP-key buffer, and a buffer that would overflow goes to dst with one atomic on
+// the global counter, so a sparse compaction takes one atomic per CAP keys instead of one per
+// warp and vector row.  Every lane of the warp makes the same calls; count is the same in all
+// lanes.  Positions at or beyond `cap` are not written.
+template <class U, int E, int CAP>
+struct WarpStage {
+  U* buf;
+  uint32_t count;
+  U* __restrict__ dst;
+  unsigned long long* counter;
+  int64_t cap;
+
+  __device__ __forceinline__ void flush() {
+    if (count == 0u) return;
+    const int lane = threadIdx.x & 31;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(counter, (unsigned long long)count);
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    for (uint32_t j = lane; j < count; j += 32)
+      if (int64_t(base + j) < cap) dst[base + j] = buf[j];
+    __syncwarp();
+    count = 0u;
+  }
+
+  __device__ __forceinline__ void add(const U* k, uint32_t take) {
+    static_assert(32 * E <= CAP, "one call must fit an empty buffer");
+    const int lane = threadIdx.x & 31;
+    const uint32_t c = __popc(take);
+    uint32_t incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    if (total == 0u) return;  // uniform over the warp
+    if (count + total > uint32_t(CAP)) flush();
+    uint32_t pos = count + incl - c;
+#pragma unroll
+    for (int e = 0; e < E; e++)
+      if ((take >> e) & 1u) buf[pos++] = k[e];
+    count += total;
+    __syncwarp();  // the keys are in the buffer before any lane flushes it
+  }
+};
 
 // Histogram of the digit at `shift` over keys whose ordered bits match (prefix, mask).
 template <class U, int KIND>
-__global__ void __launch_bounds__(SEL_NT) select_hist_kernel(const U* __restrict__ keys, const int64_t* n_ptr,
+__global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) select_hist_kernel(const U* __restrict__ keys, const int64_t* n_ptr,
                                                              int64_t n_fixed, SelectState* st, int shift) {
   using KO = KeyOrder<U, KIND>;
+  constexpr int E = int(16 / sizeof(U));
   __shared__ uint32_t sh[256 * SEL_COPIES];
   const int tid = threadIdx.x, lane = tid & 31;
   for (int i = tid; i < 256 * SEL_COPIES; i += SEL_NT) sh[i] = 0;
   __syncthreads();
   const int64_t n = n_ptr ? *n_ptr : n_fixed;
   const U prefix = U(st->prefix), mask = U(st->mask);
-  const int64_t stride = int64_t(gridDim.x) * SEL_NT;
-  for (int64_t i = int64_t(blockIdx.x) * SEL_NT + tid; i < n; i += stride) {
-    const U o = KO::to_ordered(keys[i]);
-    if ((o & mask) == prefix) atomicAdd(&sh[((uint32_t(o >> shift) & 0xFFu) * SEL_COPIES) + lane], 1u);
-  }
+  visit_keys<U>(keys, n, [&](const U* k, int nv) {
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const U o = KO::to_ordered(k[e]);
+      if (e < nv && (o & mask) == prefix) atomicAdd(&sh[((uint32_t(o >> shift) & 0xFFu) * SEL_COPIES) + lane], 1u);
+    }
+  });
   __syncthreads();
   for (int b = tid; b < 256; b += SEL_NT) {
     uint32_t c = 0;
@@ -109,30 +241,35 @@ __global__ void select_pick_kernel(SelectState* st, int shift, int last) {
   if (tid < 256) st->hist[tid] = 0;
 }
 
-// Copies the keys whose ordered top byte matches the level-0 prefix into `cand`.
+// Copies the keys whose ordered top byte matches the level-0 prefix into `cand`.  With `out`
+// (top-k): the keys above that bin, all among the k largest, go to out[0..) through
+// st->gathered at once (fewer than k of them: the selected rank lies in the bin).
 template <class U, int KIND>
-__global__ void __launch_bounds__(SEL_NT) select_compact_kernel(const U* __restrict__ keys, int64_t n,
-                                                                U* __restrict__ cand, SelectState* st) {
+__global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) select_compact_kernel(const U* __restrict__ keys, int64_t n,
+                                                                U* __restrict__ cand, SelectState* st,
+                                                                U* __restrict__ out, int64_t k_out) {
   using KO = KeyOrder<U, KIND>;
+  constexpr int E = int(16 / sizeof(U));
+  constexpr int CAP = 1024 / int(sizeof(U));  // 1 KiB per warp and buffer
+  __shared__ U s_buf[2][SEL_NT / 32][CAP];
+  const int warp = threadIdx.x >> 5;
   const U prefix = U(st->prefix), mask = U(st->mask);
-  const int lane = threadIdx.x & 31;
-  const int64_t stride = int64_t(gridDim.x) * SEL_NT;
-  // warp-uniform loop bounds: every lane reaches the ballot
-  for (int64_t base = int64_t(blockIdx.x) * SEL_NT + (threadIdx.x - lane); base < n; base += stride) {
-    const int64_t i = base + lane;
-    U k = U(0);
-    bool take = false;
-    if (i < n) {
-      k = keys[i];
-      take = (KO::to_ordered(k) & mask) == prefix;
+  WarpStage<U, E, CAP> to_cand{s_buf[0][warp], 0u, cand, reinterpret_cast<unsigned long long*>(&st->cand_count),
+                               INT64_MAX};
+  WarpStage<U, E, CAP> to_out{s_buf[1][warp], 0u, out, &st->gathered, k_out};
+  visit_keys<U>(keys, n, [&](const U* k, int nv) {
+    uint32_t take = 0u, above = 0u;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const U top = KO::to_ordered(k[e]) & mask;
+      if (e < nv && top == prefix) take |= 1u << e;
+      if (e < nv && top > prefix) above |= 1u << e;
     }
-    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, take);
-    if (bal == 0u) continue;
-    unsigned long long slot = 0;
-    if (lane == 0) slot = atomicAdd(reinterpret_cast<unsigned long long*>(&st->cand_count), (unsigned long long)__popc(bal));
-    slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
-    if (take) cand[slot + __popc(bal & lanemask_lt())] = k;
-  }
+    to_cand.add(k, take);
+    if (out) to_out.add(k, above);
+  });
+  to_cand.flush();
+  if (out) to_out.flush();
 }
 
 // ---- stable three-way partition around the selected key -----------------------------
@@ -153,6 +290,7 @@ __global__ void __launch_bounds__(PART_NT) partition_count_kernel(const U* __res
   __syncthreads();
   const int64_t base = int64_t(blockIdx.x) * PART_TILE;
   uint32_t l = 0, e = 0, g = 0;
+#pragma unroll
   for (int i = threadIdx.x; i < PART_TILE; i += PART_NT) {
     const int64_t j = base + i;
     if (j < n) {
@@ -200,26 +338,48 @@ static __global__ void partition_scan_kernel(uint32_t* tile_counts, int64_t tile
   }
 }
 
+// Each thread takes PART_KPT consecutive keys (blocked: 16-byte loads when the keys are
+// aligned), so a block scan of the per-thread class counts gives stable positions.  The tile is
+// staged in shared memory in class order and written by consecutive threads to consecutive
+// positions of each class's run.
 template <class U, int KIND>
 __global__ void __launch_bounds__(PART_NT) partition_scatter_kernel(const U* __restrict__ keys, int64_t n,
                                                                     const SelectState* st,
                                                                     const uint32_t* tile_starts,
                                                                     U* __restrict__ out) {
-  // Each thread takes PART_KPT consecutive keys (blocked), so a block scan of the per-thread
-  // class counts gives stable positions.
+  constexpr int E = int(16 / sizeof(U));
+  static_assert(PART_KPT % E == 0, "whole vectors per thread");
   __shared__ uint32_t wsum[3][PART_NT / 32];
+  __shared__ uint32_t s_at[3];  // start of each class's run in the staged tile
+  __shared__ U s_k[PART_TILE];
   const U v = U(st->prefix);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int64_t base = int64_t(blockIdx.x) * PART_TILE + int64_t(tid) * PART_KPT;
+  const int64_t tile0 = int64_t(blockIdx.x) * PART_TILE;
+  const int64_t base = tile0 + int64_t(tid) * PART_KPT;
+  const int tile_n = int(n - tile0 < PART_TILE ? n - tile0 : PART_TILE);
   U k[PART_KPT];
   uint8_t cls[PART_KPT];
   uint32_t cnt[3] = {0, 0, 0};
+  const bool vec = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0 && base + PART_KPT <= n;
+  if (vec) {
+    union {
+      uint4 v;
+      U k[E];
+    } u;
+#pragma unroll
+    for (int q = 0; q < PART_KPT / E; q++) {
+      u.v = __ldg(reinterpret_cast<const uint4*>(keys + base) + q);
+#pragma unroll
+      for (int e = 0; e < E; e++) k[q * E + e] = u.k[e];
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < PART_KPT; i++) k[i] = base + i < n ? keys[base + i] : U(0);
+  }
 #pragma unroll
   for (int i = 0; i < PART_KPT; i++) {
-    const int64_t j = base + i;
     cls[i] = 3;
-    if (j < n) {
-      k[i] = keys[j];
+    if (base + i < n) {
       cls[i] = uint8_t(part_class<U, KIND>(k[i], v));
       cnt[cls[i]]++;
     }
@@ -237,50 +397,56 @@ __global__ void __launch_bounds__(PART_NT) partition_scatter_kernel(const U* __r
     if (lane == 31) wsum[c][warp] = incl;
   }
   __syncthreads();
+  if (tid == 0) {
+    uint32_t at = 0;
+    for (int c = 0; c < 3; c++) {
+      s_at[c] = at;
+      for (int w = 0; w < PART_NT / 32; w++) at += wsum[c][w];
+    }
+  }
+  __syncthreads();
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     uint32_t wb = 0;
     for (int w = 0; w < warp; w++) wb += wsum[c][w];
-    excl[c] += wb + tile_starts[int64_t(blockIdx.x) * 3 + c];
+    excl[c] += wb + s_at[c];
   }
 #pragma unroll
-  for (int i = 0; i < PART_KPT; i++) {
-    if (cls[i] < 3) {
-      const uint32_t pos = excl[cls[i]]++;
-      if (int64_t(pos) < n) out[pos] = k[i];
-    }
+  for (int i = 0; i < PART_KPT; i++)
+    if (cls[i] < 3) s_k[excl[cls[i]]++] = k[i];
+  __syncthreads();
+  const uint32_t at1 = s_at[1], at2 = s_at[2];
+  const uint32_t* ts = tile_starts + int64_t(blockIdx.x) * 3;
+  const int64_t o0 = ts[0], o1 = int64_t(ts[1]) - at1, o2 = int64_t(ts[2]) - at2;
+  for (int j = tid; j < tile_n; j += PART_NT) {
+    const uint32_t uj = uint32_t(j);
+    const int64_t pos = (uj < at1 ? o0 : (uj < at2 ? o1 : o2)) + j;
+    if (pos < n) out[pos] = s_k[j];
   }
 }
 
 // ---- the k largest: keys > v compacted, then copies of v ------------------------------
+// The keys above the level-0 bin are already in out (select_compact_kernel); this appends the
+// candidates > v (the level-0 bin's keys) and fills the rest with copies of v.
 template <class U, int KIND>
-__global__ void __launch_bounds__(SEL_NT) topk_gather_kernel(const U* __restrict__ keys, int64_t n, int64_t k,
+__global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) topk_gather_kernel(const U* __restrict__ cand, int64_t k,
                                                              SelectState* st, U* __restrict__ out) {
-  unsigned long long* counter = &st->gathered;
   using KO = KeyOrder<U, KIND>;
+  constexpr int E = int(16 / sizeof(U));
   const U v = U(st->prefix);
+  const int64_t n = st->n_total;
   int64_t greater = n - st->less - st->eq;
   greater = greater < 0 ? 0 : greater;  // never index below out[0]
-  const int lane = threadIdx.x & 31;
-  const int64_t stride = int64_t(gridDim.x) * SEL_NT;
-  for (int64_t b = int64_t(blockIdx.x) * SEL_NT + (threadIdx.x - lane); b < n; b += stride) {
-    const int64_t i = b + lane;
-    U key = U(0);
-    bool take = false;
-    if (i < n) {
-      key = keys[i];
-      take = KO::to_ordered(key) > v;
-    }
-    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, take);
-    if (bal == 0u) continue;
-    unsigned long long slot = 0;
-    if (lane == 0) slot = atomicAdd(counter, (unsigned long long)__popc(bal));
-    slot = __shfl_sync(0xFFFFFFFFu, slot, 0);
-    const unsigned long long pos = slot + __popc(bal & lanemask_lt());
-    if (take && int64_t(pos) < k) out[pos] = key;
-  }
+  visit_keys<U>(cand, st->cand_count, [&](const U* kk, int nv) {
+    uint32_t take = 0u;
+#pragma unroll
+    for (int e = 0; e < E; e++)
+      if (e < nv && KO::to_ordered(kk[e]) > v) take |= 1u << e;
+    warp_append<U, E>(kk, take, out, &st->gathered, k);
+  });
   // copies of the selected key fill the rest (greater <= k by construction)
   const U vraw = KO::from_ordered(v);
+  const int64_t stride = int64_t(gridDim.x) * SEL_NT;
   const int64_t gtid = int64_t(blockIdx.x) * SEL_NT + threadIdx.x;
   for (int64_t j = greater + gtid; j < k; j += stride) out[j] = vraw;
 }

@@ -8,10 +8,21 @@
 
 namespace hpcs {
 
+// Grid of the passes over the keys: SEL_CTAS_PER_SM CTAs per SM, fewer for small inputs.
+inline int select_grid(hpcs_ctx* ctx, int64_t n, int key_bytes) {
+  const int64_t per_cta = int64_t(SEL_NT) * SEL_VPT * (16 / key_bytes);
+  const int64_t want = (n + per_cta - 1) / per_cta;
+  const int64_t cap = int64_t(ctx->sms) * SEL_CTAS_PER_SM;
+  return int(want < 1 ? 1 : (want > cap ? cap : want));
+}
+
 // Radix select of the key of 0-based rank `rank` among n keys at device pointer d.  Leaves
 // the SelectState in ctx->aux1 (prefix = the ordered bits of the selected key, less/eq counts).
+// With top_out (top-k of the k = n - rank largest), the level-0 compaction also writes the
+// keys above the level-0 bin to top_out.
 template <class U, int KIND>
-inline int enqueue_select(hpcs_ctx* ctx, const U* d, int64_t n, int64_t rank, cudaStream_t s, SelectState** out) {
+inline int enqueue_select(hpcs_ctx* ctx, const U* d, int64_t n, int64_t rank, cudaStream_t s, SelectState** out,
+                          U* top_out = nullptr) {
   constexpr int BITS = int(sizeof(U) * 8);
   constexpr int LEVELS = BITS / 8;
   int rc;
@@ -20,12 +31,11 @@ inline int enqueue_select(hpcs_ctx* ctx, const U* d, int64_t n, int64_t rank, cu
   SelectState* st = static_cast<SelectState*>(ctx->aux1.ptr);
   U* cand = static_cast<U*>(ctx->aux0.ptr);
   KernelTimer kt(ctx, s, HPCS_K_TOPK);
-  select_init_kernel<<<1, 256, 0, s>>>(st, rank);
-  const int64_t want = (n + SEL_NT * 4 - 1) / (SEL_NT * 4);
-  const int grid = int(want < 1 ? 1 : (want > int64_t(ctx->sms) * 2 ? int64_t(ctx->sms) * 2 : want));
+  select_init_kernel<<<1, 256, 0, s>>>(st, rank, n);
+  const int grid = select_grid(ctx, n, int(sizeof(U)));
   select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, nullptr, n, st, BITS - 8);
   select_pick_kernel<U><<<1, 256, 0, s>>>(st, BITS - 8, LEVELS == 1);
-  select_compact_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, cand, st);
+  select_compact_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, cand, st, top_out, n - rank);
   for (int l = 1; l < LEVELS; l++) {
     const int shift = BITS - 8 * (l + 1);
     select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(cand, &st->cand_count, 0, st, shift);
@@ -56,12 +66,12 @@ template <class T, class U, int KIND>
 inline int topk_largest_enqueue(hpcs_ctx* ctx, const U* d, int64_t n, int64_t k, U* out, cudaStream_t s) {
   SelectState* st = nullptr;
   int rc;
-  if ((rc = enqueue_select<U, KIND>(ctx, d, n, n - k, s, &st)) != HPCS_OK) return rc;
-  const int64_t want = (n + SEL_NT * 4 - 1) / (SEL_NT * 4);
-  const int grid = int(want < 1 ? 1 : (want > int64_t(ctx->sms) * 2 ? int64_t(ctx->sms) * 2 : want));
+  if ((rc = enqueue_select<U, KIND>(ctx, d, n, n - k, s, &st, out)) != HPCS_OK) return rc;
   {
+    // candidates: at most n of them, usually about n/256; the grid covers n
     KernelTimer kt(ctx, s, HPCS_K_TOPK);
-    topk_gather_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, k, st, out);
+    const U* cand = static_cast<const U*>(ctx->aux0.ptr);
+    topk_gather_kernel<U, KIND><<<select_grid(ctx, n, int(sizeof(U))), SEL_NT, 0, s>>>(cand, k, st, out);
     HPCS_CUDA(cudaGetLastError());
   }
   return enqueue_sort<U, KIND, NoValue>(ctx, out, nullptr, k, s);
