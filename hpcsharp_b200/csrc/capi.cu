@@ -204,7 +204,8 @@ int enqueue_count_sort(hpcs_ctx* ctx, U* d, int64_t n, uint32_t flip, cudaStream
   }
   HPCS_CUDA(cudaMemsetAsync(counts, 0, size_t(BINS) * 4, s));
   const int64_t want = (n + int64_t(COUNT_NT) * 16 - 1) / (int64_t(COUNT_NT) * 16);
-  const int hgrid = int(want < 1 ? 1 : (want > ctx->sms ? ctx->sms : want));
+  const int64_t hcap = int64_t(ctx->sms) * (BINS == 256 ? 2 : 1);  // CTAs per SM that fit the counters
+  const int hgrid = int(want < 1 ? 1 : (want > hcap ? hcap : want));
   {
     KernelTimer kt(ctx, s, HPCS_K_HISTOGRAM);
     kh<<<hgrid, COUNT_NT, smem, s>>>(d, n, flip, counts);
@@ -212,12 +213,12 @@ int enqueue_count_sort(hpcs_ctx* ctx, U* d, int64_t n, uint32_t flip, cudaStream
   }
   count_scan_kernel<BINS><<<1, COUNT_NT, 0, s>>>(counts, starts);
   HPCS_CUDA(cudaGetLastError());
-  const int64_t vecs = n / (16 / int64_t(sizeof(U))) + 1;
-  const int64_t fwant = (vecs + 255) / 256;
-  const int fgrid = int(fwant > int64_t(ctx->sms) * 16 ? int64_t(ctx->sms) * 16 : fwant);
+  const int64_t range = int64_t(COUNT_FILL_NT) * COUNT_FILL_VPT * (16 / int64_t(sizeof(U)));
+  const int64_t fwant = (n + range - 1) / range;
+  const int fgrid = int(fwant > int64_t(ctx->sms) * 8 ? int64_t(ctx->sms) * 8 : fwant);
   {
     KernelTimer kt(ctx, s, HPCS_K_FINALIZE);
-    count_fill_kernel<U><<<fgrid, 256, 0, s>>>(d, n, starts, flip);
+    count_fill_kernel<U><<<fgrid, COUNT_FILL_NT, 0, s>>>(d, n, starts, flip);
     HPCS_CUDA(cudaGetLastError());
   }
   return HPCS_OK;

@@ -165,4 +165,79 @@ __device__ __forceinline__ uint4 ldg_stream_v4(const void* p) {
   return v;
 }
 
+// Calls f(k, nv) for the keys of keys[0..n) in groups of E = 16 / sizeof(U): k holds E keys,
+// the first nv of them valid.  The 16-byte-aligned body goes as vectors, VPT per thread in
+// flight (vector j of a round at base + j*G + global thread id, G = grid threads); the
+// unaligned head (< E keys) and the ragged tail (< E keys) go to lanes 0 and 1 of the grid's
+// first warp.  Every lane of a warp makes the same calls (nv = 0 pads), so f may use warp
+// collectives.
+template <class U, int VPT, class F>
+__device__ __forceinline__ void visit_keys(const U* __restrict__ keys, int64_t n, F&& f) {
+  constexpr int E = int(16 / sizeof(U));
+  union Vec {
+    uint4 v;
+    U k[E];
+  };
+  const uintptr_t addr = reinterpret_cast<uintptr_t>(keys);
+  int64_t head = int64_t(((16u - uint32_t(addr & 15u)) & 15u) / sizeof(U));
+  if (head > n) head = n;
+  const int64_t nvec = (n - head) / E;
+  const int64_t rest = head + nvec * E;  // first key of the tail
+  const uint4* vp = reinterpret_cast<const uint4*>(keys + head);
+  const int64_t G = int64_t(gridDim.x) * blockDim.x;
+  const int64_t gtid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  for (int64_t base = 0; base < nvec; base += G * VPT) {  // uniform over the grid
+    Vec v[VPT];
+#pragma unroll
+    for (int j = 0; j < VPT; j++) {
+      const int64_t idx = base + j * G + gtid;
+      v[j].v = idx < nvec ? __ldg(vp + idx) : make_uint4(0u, 0u, 0u, 0u);
+    }
+#pragma unroll
+    for (int j = 0; j < VPT; j++) f(v[j].k, base + j * G + gtid < nvec ? E : 0);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    Vec v;
+    v.v = make_uint4(0u, 0u, 0u, 0u);
+    int nv = 0;
+    if (lane == 0) {
+      nv = int(head);
+      for (int e = 0; e < nv; e++) v.k[e] = keys[e];
+    } else if (lane == 1) {
+      nv = int(n - rest);
+      for (int e = 0; e < nv; e++) v.k[e] = keys[rest + e];
+    }
+    f(v.k, nv);
+  }
+}
+
+// Appends the keys k[e] whose bit e of `take` is set to dst at a position drawn from *counter
+// (one atomic per warp); positions at or beyond `cap` are not written.  All lanes call it.
+template <class U, int E>
+__device__ __forceinline__ void warp_append(const U* k, uint32_t take, U* __restrict__ dst,
+                                            unsigned long long* counter, int64_t cap) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t c = __popc(take);
+  uint32_t incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  if (total == 0u) return;  // uniform over the warp
+  unsigned long long base = 0;
+  if (lane == 31) base = atomicAdd(counter, (unsigned long long)total);
+  base = __shfl_sync(0xFFFFFFFFu, base, 31);
+  unsigned long long pos = base + incl - c;
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    if ((take >> e) & 1u) {
+      if (int64_t(pos) < cap) dst[pos] = k[e];
+      pos++;
+    }
+  }
+}
+
 }  // namespace hpcs

@@ -30,21 +30,24 @@ constexpr int COUNT_ROUND = 16;  // keys per thread between barriers (16-bit cou
 // exactly one thread sees each crossing; the keys go in rounds of COUNT_ROUND per thread
 // with a barrier between rounds, so before a crossing thread's subtraction lands at most one
 // round of the CTA's increments (16384) can reach the counter: it stays below 0xC000.
+// The keys are read as 16-byte vectors (visit_keys for 8-bit keys; two vectors per thread and
+// round for 16-bit keys), the unaligned head and ragged tail by the grid's first warp.
 // `flip` is the signed transform's top-bit mask (0 for unsigned keys).
 template <class T>
-__global__ void __launch_bounds__(COUNT_NT, 1) count_hist_kernel(const T* __restrict__ a, int64_t n, uint32_t flip,
-                                                                 uint32_t* __restrict__ counts) {
+__global__ void __launch_bounds__(COUNT_NT) count_hist_kernel(const T* __restrict__ a, int64_t n, uint32_t flip,
+                                                              uint32_t* __restrict__ counts) {
   constexpr int BINS = CountTraits<T>::BINS;
+  constexpr int E = int(16 / sizeof(T));
   extern __shared__ __align__(16) uint32_t sh[];
   const int tid = threadIdx.x, lane = tid & 31;
-  const int64_t stride = int64_t(gridDim.x) * COUNT_NT;
   if (BINS == 256) {
     for (int i = tid; i < 256 * 32; i += COUNT_NT) sh[i] = 0u;
     __syncthreads();
-    for (int64_t i = int64_t(blockIdx.x) * COUNT_NT + tid; i < n; i += stride) {
-      const uint32_t b = (uint32_t(a[i]) ^ flip) & 0xFFu;
-      atomicAdd(&sh[b * 32 + lane], 1u);
-    }
+    visit_keys<T, 2>(a, n, [&](const T* k, int nv) {
+#pragma unroll
+      for (int e = 0; e < E; e++)
+        if (e < nv) atomicAdd(&sh[((uint32_t(k[e]) ^ flip) & 0xFFu) * 32 + lane], 1u);
+    });
     __syncthreads();
     for (int b = tid; b < 256; b += COUNT_NT) {
       uint32_t c = 0;
@@ -55,24 +58,49 @@ __global__ void __launch_bounds__(COUNT_NT, 1) count_hist_kernel(const T* __rest
   } else {
     for (int i = tid; i < BINS / 2; i += COUNT_NT) sh[i] = 0u;
     __syncthreads();
-    const int64_t per_round = stride * COUNT_ROUND;
-    for (int64_t r0 = 0; r0 < n; r0 += per_round) {  // the same number of rounds in every thread
-#pragma unroll 4
-      for (int g = 0; g < COUNT_ROUND; g++) {
-        const int64_t i = r0 + g * stride + int64_t(blockIdx.x) * COUNT_NT + tid;
-        if (i < n) {
-          const uint32_t b = (uint32_t(a[i]) ^ flip) & 0xFFFFu;
-          const uint32_t sh16 = (b & 1u) << 4;
-          const uint32_t inc = 1u << sh16;
-          const uint32_t old = atomicAdd(&sh[b >> 1], inc);
-          if ((old + inc) & ~old & 0x80008000u) {
-            atomicSub(&sh[b >> 1], 0x8000u << sh16);
-            atomicAdd(counts + b, 0x8000u);
-          }
-        }
+    auto bump = [&](uint32_t key) {
+      const uint32_t b = (key ^ flip) & 0xFFFFu;
+      const uint32_t sh16 = (b & 1u) << 4;
+      const uint32_t inc = 1u << sh16;
+      const uint32_t old = atomicAdd(&sh[b >> 1], inc);
+      if ((old + inc) & ~old & 0x80008000u) {
+        atomicSub(&sh[b >> 1], 0x8000u << sh16);
+        atomicAdd(counts + b, 0x8000u);
       }
+    };
+    union Vec {
+      uint4 v;
+      T k[E];
+    };
+    constexpr int VPR = COUNT_ROUND / E;  // vectors per thread and round
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(a);
+    int64_t head = int64_t(((16u - uint32_t(addr & 15u)) & 15u) / sizeof(T));
+    if (head > n) head = n;
+    const int64_t nvec = (n - head) / E;
+    const int64_t rest = head + nvec * E;
+    const uint4* vp = reinterpret_cast<const uint4*>(a + head);
+    const int64_t G = int64_t(gridDim.x) * COUNT_NT;
+    const int64_t gtid = int64_t(blockIdx.x) * COUNT_NT + tid;
+    for (int64_t base = 0; base < nvec; base += G * VPR) {  // the same number of rounds in every thread
+      Vec v[VPR];
+#pragma unroll
+      for (int j = 0; j < VPR; j++) {
+        const int64_t idx = base + j * G + gtid;
+        v[j].v = idx < nvec ? __ldg(vp + idx) : make_uint4(0u, 0u, 0u, 0u);
+      }
+#pragma unroll
+      for (int j = 0; j < VPR; j++)
+        if (base + j * G + gtid < nvec) {
+#pragma unroll
+          for (int e = 0; e < E; e++) bump(uint32_t(v[j].k[e]));
+        }
       __syncthreads();
     }
+    if (blockIdx.x == 0 && tid == 0) {  // fewer than 2E keys outside the vectors
+      for (int64_t i = 0; i < head; i++) bump(uint32_t(a[i]));
+      for (int64_t i = rest; i < n; i++) bump(uint32_t(a[i]));
+    }
+    __syncthreads();
     for (int w = tid; w < BINS / 2; w += COUNT_NT) {
       const uint32_t v = sh[w];
       if (v & 0xFFFFu) atomicAdd(counts + 2 * w, v & 0xFFFFu);
@@ -112,18 +140,27 @@ __global__ void __launch_bounds__(COUNT_NT) count_scan_kernel(const uint32_t* __
   if (tid == COUNT_NT - 1) starts[BINS] = base + incl;
 }
 
-// Fills out[i] with the value v whose run [starts[v], starts[v+1]) holds i.  Each thread
-// writes 16-byte vectors: it finds the bin of the vector's first element by binary search over
-// the starts, then walks forward across bin boundaries.  The ragged tail is written with
-// scalar stores.  `flip` maps a bin back to its raw bits.
+// Fills out[i] with the value v whose run [starts[v], starts[v+1]) holds i.  Each CTA takes
+// ranges of COUNT_FILL_KEYS outputs (grid-stride): it finds the bins of the range's first and
+// last output by binary search over the starts, copies those bins' starts into shared memory
+// (when there are at most COUNT_FILL_SMEM of them; otherwise the searches below stay in
+// global memory), and each thread writes 16-byte vectors: the bin of a vector's first element
+// by binary search over the copied starts, then a walk across bin boundaries.  Unaligned
+// outputs and the ragged end are written by scalar stores.  `flip` maps a bin back to its raw
+// bits.
+constexpr int COUNT_FILL_NT = 256;
+constexpr int COUNT_FILL_VPT = 16;  // vectors per thread and range
+constexpr int COUNT_FILL_SMEM = 2048;
+
 template <class T>
-__global__ void __launch_bounds__(256) count_fill_kernel(T* __restrict__ out, int64_t n,
-                                                         const int64_t* __restrict__ starts, uint32_t flip) {
+__global__ void __launch_bounds__(COUNT_FILL_NT) count_fill_kernel(T* __restrict__ out, int64_t n,
+                                                                   const int64_t* __restrict__ starts, uint32_t flip) {
   constexpr int BINS = CountTraits<T>::BINS;
   constexpr int VEC = 16 / int(sizeof(T));
-  const int64_t nvec = n / VEC;
-  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-  auto bin_of = [&](int64_t i) {  // largest v with starts[v] <= i (runs may be empty)
+  constexpr int64_t R = int64_t(COUNT_FILL_NT) * COUNT_FILL_VPT * VEC;  // outputs per range
+  __shared__ int64_t s_st[COUNT_FILL_SMEM + 1];
+  __shared__ int s_lo, s_cnt;
+  auto bin_of_global = [&](int64_t i) {  // largest v with starts[v] <= i (runs may be empty)
     int lo = 0, hi = BINS - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
@@ -133,36 +170,73 @@ __global__ void __launch_bounds__(256) count_fill_kernel(T* __restrict__ out, in
     return lo;
   };
   const bool aligned = (reinterpret_cast<uintptr_t>(out) & 15) == 0;
-  for (int64_t vi = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; vi < nvec + 1; vi += stride) {
-    const int64_t first = vi * VEC;
-    if (first >= n) break;
-    int v = bin_of(first);
-    int64_t next = starts[v + 1];
-    if (vi < nvec && aligned) {
-      union {
-        uint4 u;
-        T e[VEC];
-      } pack;
-#pragma unroll
-      for (int q = 0; q < VEC; q++) {
-        const int64_t i = first + q;
-        while (i >= next && v < BINS - 1) {
-          v++;
-          next = starts[v + 1];
+  const int tid = threadIdx.x;
+  for (int64_t a = int64_t(blockIdx.x) * R; a < n; a += int64_t(gridDim.x) * R) {
+    const int64_t e = a + R < n ? a + R : n;
+    if (tid == 0) {
+      const int lo = bin_of_global(a), hi = bin_of_global(e - 1);
+      s_lo = lo;
+      s_cnt = hi - lo + 2;  // starts[lo .. hi + 1]
+    }
+    __syncthreads();
+    const int lo = s_lo, cnt = s_cnt;
+    const bool local = cnt <= COUNT_FILL_SMEM + 1;
+    if (local)
+      for (int i = tid; i < cnt; i += COUNT_FILL_NT) s_st[i] = starts[lo + i];
+    __syncthreads();
+    // bin of output i in [a, e) and the start of the next bin
+    auto find = [&](int64_t i, int& v, int64_t& next) {
+      if (local) {
+        int l = 0, h = cnt - 2;
+        while (l < h) {
+          const int mid = (l + h + 1) >> 1;
+          if (s_st[mid] <= i) l = mid;
+          else h = mid - 1;
         }
-        pack.e[q] = T(uint32_t(v) ^ flip);
+        v = lo + l;
+        next = s_st[l + 1];
+      } else {
+        v = bin_of_global(i);
+        next = starts[v + 1];
       }
-      reinterpret_cast<uint4*>(out)[vi] = pack.u;
-    } else {
-      const int64_t last = vi < nvec ? first + VEC : n;
-      for (int64_t i = first; i < last; i++) {
-        while (i >= next && v < BINS - 1) {
-          v++;
-          next = starts[v + 1];
+    };
+    auto advance = [&](int& v, int64_t& next) {
+      v++;
+      next = local ? s_st[v - lo + 1] : starts[v + 1];
+    };
+    if (aligned) {
+      const int64_t nvec = (e - a) / VEC;  // whole vectors of the range (a is a multiple of VEC)
+      for (int64_t q = tid; q < nvec; q += COUNT_FILL_NT) {
+        const int64_t first = a + q * VEC;
+        int v;
+        int64_t next;
+        find(first, v, next);
+        union {
+          uint4 u;
+          T e[VEC];
+        } pack;
+#pragma unroll
+        for (int r = 0; r < VEC; r++) {
+          while (first + r >= next && v < BINS - 1) advance(v, next);
+          pack.e[r] = T(uint32_t(v) ^ flip);
         }
+        reinterpret_cast<uint4*>(out)[first / VEC] = pack.u;
+      }
+      for (int64_t i = a + nvec * VEC + tid; i < e; i += COUNT_FILL_NT) {
+        int v;
+        int64_t next;
+        find(i, v, next);
+        out[i] = T(uint32_t(v) ^ flip);
+      }
+    } else {
+      for (int64_t i = a + tid; i < e; i += COUNT_FILL_NT) {
+        int v;
+        int64_t next;
+        find(i, v, next);
         out[i] = T(uint32_t(v) ^ flip);
       }
     }
+    __syncthreads();  // the copied starts are read before the next range replaces them
   }
 }
 

@@ -12,7 +12,8 @@
 // levels histogram only candidates that match the prefix chosen so far.  A one-block "pick"
 // kernel after each histogram advances the device-side SelectState, so nothing returns to the
 // host between levels.  The passes over all n keys read them with 16-byte loads, several in
-// flight per thread (visit_keys); compactions take one atomic per warp and vector row.
+// flight per thread (visit_keys); compactions stage kept keys per warp in shared memory and
+// take one global atomic per 1 KiB of them.
 //
 // Rearrangement: a stable three-way partition (keys < v, == v, > v around the selected key v)
 // in three kernels -- per-tile class counts, a one-block scan, a stable per-tile scatter.
@@ -58,81 +59,6 @@ constexpr int SEL_NT = 512;
 constexpr int SEL_COPIES = 32;
 constexpr int SEL_VPT = 4;  // 16-byte vectors in flight per thread
 constexpr int SEL_CTAS_PER_SM = 4;
-
-// Calls f(k, nv) for the keys of keys[0..n) in groups of E = 16 / sizeof(U): k holds E keys,
-// the first nv of them valid.  The 16-byte-aligned body goes as vectors, SEL_VPT per thread in
-// flight (vector j of a round at base + j*G + global thread id, G = grid threads); the
-// unaligned head (< E keys) and the ragged tail (< E keys) go to lanes 0 and 1 of the grid's
-// first warp.  Every lane of a warp makes the same calls (nv = 0 pads), so f may use warp
-// collectives.
-template <class U, class F>
-__device__ __forceinline__ void visit_keys(const U* __restrict__ keys, int64_t n, F&& f) {
-  constexpr int E = int(16 / sizeof(U));
-  union Vec {
-    uint4 v;
-    U k[E];
-  };
-  const uintptr_t addr = reinterpret_cast<uintptr_t>(keys);
-  int64_t head = int64_t(((16u - uint32_t(addr & 15u)) & 15u) / sizeof(U));
-  if (head > n) head = n;
-  const int64_t nvec = (n - head) / E;
-  const int64_t rest = head + nvec * E;  // first key of the tail
-  const uint4* vp = reinterpret_cast<const uint4*>(keys + head);
-  const int64_t G = int64_t(gridDim.x) * blockDim.x;
-  const int64_t gtid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  for (int64_t base = 0; base < nvec; base += G * SEL_VPT) {  // uniform over the grid
-    Vec v[SEL_VPT];
-#pragma unroll
-    for (int j = 0; j < SEL_VPT; j++) {
-      const int64_t idx = base + j * G + gtid;
-      v[j].v = idx < nvec ? __ldg(vp + idx) : make_uint4(0u, 0u, 0u, 0u);
-    }
-#pragma unroll
-    for (int j = 0; j < SEL_VPT; j++) f(v[j].k, base + j * G + gtid < nvec ? E : 0);
-  }
-  if (blockIdx.x == 0 && threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    Vec v;
-    v.v = make_uint4(0u, 0u, 0u, 0u);
-    int nv = 0;
-    if (lane == 0) {
-      nv = int(head);
-      for (int e = 0; e < nv; e++) v.k[e] = keys[e];
-    } else if (lane == 1) {
-      nv = int(n - rest);
-      for (int e = 0; e < nv; e++) v.k[e] = keys[rest + e];
-    }
-    f(v.k, nv);
-  }
-}
-
-// Appends the keys k[e] whose bit e of `take` is set to dst at a position drawn from *counter
-// (one atomic per warp); positions at or beyond `cap` are not written.  All lanes call it.
-template <class U, int E>
-__device__ __forceinline__ void warp_append(const U* k, uint32_t take, U* __restrict__ dst,
-                                            unsigned long long* counter, int64_t cap) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t c = __popc(take);
-  uint32_t incl = c;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-    if (lane >= o) incl += y;
-  }
-  const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-  if (total == 0u) return;  // uniform over the warp
-  unsigned long long base = 0;
-  if (lane == 31) base = atomicAdd(counter, (unsigned long long)total);
-  base = __shfl_sync(0xFFFFFFFFu, base, 31);
-  unsigned long long pos = base + incl - c;
-#pragma unroll
-  for (int e = 0; e < E; e++) {
-    if ((take >> e) & 1u) {
-      if (int64_t(pos) < cap) dst[pos] = k[e];
-      pos++;
-    }
-  }
-}
 
 // Per-warp staging of appended keys in shared memory: a warp scan places each lane's keys in
 // the warp's CAP-key buffer, and a buffer that would overflow goes to dst with one atomic on
@@ -193,7 +119,7 @@ __global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) select_hist_kernel(co
   __syncthreads();
   const int64_t n = n_ptr ? *n_ptr : n_fixed;
   const U prefix = U(st->prefix), mask = U(st->mask);
-  visit_keys<U>(keys, n, [&](const U* k, int nv) {
+  visit_keys<U, SEL_VPT>(keys, n, [&](const U* k, int nv) {
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const U o = KO::to_ordered(k[e]);
@@ -257,7 +183,7 @@ __global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) select_compact_kernel
   WarpStage<U, E, CAP> to_cand{s_buf[0][warp], 0u, cand, reinterpret_cast<unsigned long long*>(&st->cand_count),
                                INT64_MAX};
   WarpStage<U, E, CAP> to_out{s_buf[1][warp], 0u, out, &st->gathered, k_out};
-  visit_keys<U>(keys, n, [&](const U* k, int nv) {
+  visit_keys<U, SEL_VPT>(keys, n, [&](const U* k, int nv) {
     uint32_t take = 0u, above = 0u;
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -437,7 +363,7 @@ __global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) topk_gather_kernel(co
   const int64_t n = st->n_total;
   int64_t greater = n - st->less - st->eq;
   greater = greater < 0 ? 0 : greater;  // never index below out[0]
-  visit_keys<U>(cand, st->cand_count, [&](const U* kk, int nv) {
+  visit_keys<U, SEL_VPT>(cand, st->cand_count, [&](const U* kk, int nv) {
     uint32_t take = 0u;
 #pragma unroll
     for (int e = 0; e < E; e++)
