@@ -87,6 +87,7 @@ struct WarpStage {
 
   __device__ __forceinline__ void add(const U* k, uint32_t take) {
     static_assert(32 * E <= CAP, "one call must fit an empty buffer");
+    if (__ballot_sync(0xFFFFFFFFu, take != 0u) == 0u) return;  // nothing kept by the warp
     const int lane = threadIdx.x & 31;
     const uint32_t c = __popc(take);
     uint32_t incl = c;
@@ -234,6 +235,8 @@ __global__ void __launch_bounds__(PART_NT) partition_count_kernel(const U* __res
 }
 
 // One block: tile_counts[t][c] -> exclusive start of tile t's class-c keys in the output.
+// Each thread takes PART_SCAN_PER consecutive tiles per step.
+constexpr int PART_SCAN_PER = 4;
 static __global__ void partition_scan_kernel(uint32_t* tile_counts, int64_t tiles, const SelectState* st, int64_t n) {
   __shared__ int64_t carry[3];
   __shared__ int64_t wsum[3][32];
@@ -243,24 +246,48 @@ static __global__ void partition_scan_kernel(uint32_t* tile_counts, int64_t tile
     carry[tid] = tid == 0 ? 0 : (tid == 1 ? less : less + eq);
   }
   __syncthreads();
-  for (int64_t b0 = 0; b0 < tiles; b0 += 1024) {
-    const int64_t t = b0 + tid;
+  for (int64_t b0 = 0; b0 < tiles; b0 += 1024 * PART_SCAN_PER) {
+    const int64_t t0 = b0 + int64_t(tid) * PART_SCAN_PER;
+    uint32_t v[3][PART_SCAN_PER];
+    int64_t sum[3];
+#pragma unroll
     for (int c = 0; c < 3; c++) {
-      const int64_t v = t < tiles ? int64_t(tile_counts[t * 3 + c]) : 0;
-      int64_t incl = v;
-      for (int o = 1; o < 32; o <<= 1) {
-        const int64_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= o) incl += y;
+      sum[c] = 0;
+#pragma unroll
+      for (int q = 0; q < PART_SCAN_PER; q++) {
+        v[c][q] = t0 + q < tiles ? tile_counts[(t0 + q) * 3 + c] : 0u;
+        sum[c] += v[c][q];
       }
-      if (lane == 31) wsum[c][warp] = incl;
-      __syncthreads();
-      int64_t wb = 0;
-      for (int w = 0; w < warp; w++) wb += wsum[c][w];
-      if (t < tiles) tile_counts[t * 3 + c] = uint32_t(carry[c] + wb + incl - v);
-      __syncthreads();
-      if (tid == 1023) carry[c] += wb + incl;
-      __syncthreads();
     }
+    int64_t incl[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      incl[c] = sum[c];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(0xFFFFFFFFu, incl[c], o);
+        if (lane >= o) incl[c] += y;
+      }
+      if (lane == 31) wsum[c][warp] = incl[c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      int64_t run = carry[c] + incl[c] - sum[c];
+      for (int w = 0; w < warp; w++) run += wsum[c][w];
+#pragma unroll
+      for (int q = 0; q < PART_SCAN_PER; q++) {
+        if (t0 + q < tiles) tile_counts[(t0 + q) * 3 + c] = uint32_t(run);
+        run += v[c][q];
+      }
+    }
+    __syncthreads();
+    if (tid < 3) {
+      int64_t tot = 0;
+      for (int w = 0; w < 32; w++) tot += wsum[tid][w];
+      carry[tid] += tot;
+    }
+    __syncthreads();
   }
 }
 
@@ -277,7 +304,9 @@ __global__ void __launch_bounds__(PART_NT) partition_scatter_kernel(const U* __r
   static_assert(PART_KPT % E == 0, "whole vectors per thread");
   __shared__ uint32_t wsum[3][PART_NT / 32];
   __shared__ uint32_t s_at[3];  // start of each class's run in the staged tile
-  __shared__ U s_k[PART_TILE];
+  // staged slot j lives at j + j/32: lanes writing about PART_KPT/2 slots apart land in
+  // different banks
+  __shared__ U s_k[PART_TILE + PART_TILE / 32];
   const U v = U(st->prefix);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t tile0 = int64_t(blockIdx.x) * PART_TILE;
@@ -337,9 +366,14 @@ __global__ void __launch_bounds__(PART_NT) partition_scatter_kernel(const U* __r
     for (int w = 0; w < warp; w++) wb += wsum[c][w];
     excl[c] += wb + s_at[c];
   }
+  uint32_t e0 = excl[0], e1 = excl[1], e2 = excl[2];  // next slot per class (no dynamic index)
 #pragma unroll
-  for (int i = 0; i < PART_KPT; i++)
-    if (cls[i] < 3) s_k[excl[cls[i]]++] = k[i];
+  for (int i = 0; i < PART_KPT; i++) {
+    if (cls[i] < 3) {
+      const uint32_t j = cls[i] == 0 ? e0++ : (cls[i] == 1 ? e1++ : e2++);
+      s_k[j + (j >> 5)] = k[i];
+    }
+  }
   __syncthreads();
   const uint32_t at1 = s_at[1], at2 = s_at[2];
   const uint32_t* ts = tile_starts + int64_t(blockIdx.x) * 3;
@@ -347,7 +381,7 @@ __global__ void __launch_bounds__(PART_NT) partition_scatter_kernel(const U* __r
   for (int j = tid; j < tile_n; j += PART_NT) {
     const uint32_t uj = uint32_t(j);
     const int64_t pos = (uj < at1 ? o0 : (uj < at2 ? o1 : o2)) + j;
-    if (pos < n) out[pos] = s_k[j];
+    if (pos < n) out[pos] = s_k[j + (j >> 5)];
   }
 }
 
