@@ -135,37 +135,50 @@ __global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) select_hist_kernel(co
   }
 }
 
-// One block: choose the bin holding st->rank, advance the prefix, clear the histogram.
+// One block of 256 threads: choose the bin holding st->rank (a scan of the 256 counts, the
+// thread whose bin spans the rank records it), advance the prefix, clear the histogram.
 // last != 0: record how many keys equal the selected key.
 template <class U>
-__global__ void select_pick_kernel(SelectState* st, int shift, int last) {
-  __shared__ uint32_t h[256];
-  __shared__ int64_t cum[257];
-  const int tid = threadIdx.x;
-  if (tid < 256) h[tid] = st->hist[tid];
-  __syncthreads();
+__global__ void __launch_bounds__(256) select_pick_kernel(SelectState* st, int shift, int last) {
+  __shared__ int64_t s_w[8];
+  __shared__ int s_bin;
+  __shared__ int64_t s_excl, s_cnt;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int64_t c = st->hist[tid];
+  int64_t incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_w[warp] = incl;
   if (tid == 0) {
-    int64_t run = 0;
-    for (int b = 0; b < 256; b++) {
-      cum[b] = run;
-      run += h[b];
-    }
-    cum[256] = run;
-    const int64_t r = st->rank;
-    int bin = 255;
-    for (int b = 0; b < 256; b++)
-      if (r < cum[b + 1]) {
-        bin = b;
-        break;
-      }
-    st->prefix |= uint64_t(bin) << shift;
-    st->mask |= uint64_t(0xFF) << shift;
-    st->rank = r - cum[bin];
-    st->less += cum[bin];
-    if (last) st->eq = h[bin];
+    s_bin = -1;
+    s_excl = 0;
+    s_cnt = 0;
   }
   __syncthreads();
-  if (tid < 256) st->hist[tid] = 0;
+  int64_t base = 0;
+  for (int w = 0; w < warp; w++) base += s_w[w];
+  const int64_t excl = base + incl - c;
+  const int64_t r = st->rank;
+  // the bins' ranges [excl, excl + c) are disjoint: at most one thread matches; a rank past
+  // every key (not reachable through the entry points) falls to bin 255
+  if ((c > 0 && r >= excl && r < excl + c) || (tid == 255 && r >= excl + c)) {
+    s_bin = tid;
+    s_excl = excl;
+    s_cnt = c;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const int bin = s_bin < 0 ? 255 : s_bin;
+    st->prefix |= uint64_t(bin) << shift;
+    st->mask |= uint64_t(0xFF) << shift;
+    st->rank = r - s_excl;
+    st->less += s_excl;
+    if (last) st->eq = s_cnt;
+  }
+  st->hist[tid] = 0;
 }
 
 // Copies the keys whose ordered top byte matches the level-0 prefix into `cand`.  With `out`
