@@ -211,14 +211,18 @@ int enqueue_count_sort(hpcs_ctx* ctx, U* d, int64_t n, uint32_t flip, cudaStream
     kh<<<hgrid, COUNT_NT, smem, s>>>(d, n, flip, counts);
     HPCS_CUDA(cudaGetLastError());
   }
-  count_scan_kernel<BINS><<<1, COUNT_NT, 0, s>>>(counts, starts);
+  const int64_t range = count_fill_range<U>();
+  const int64_t ranges = (n + range - 1) / range;
+  if ((rc = ensure(ctx, ctx->aux1, size_t(ranges) * 2 * 4)) != HPCS_OK) return rc;
+  int32_t* range_lo = static_cast<int32_t*>(ctx->aux1.ptr);
+  int32_t* range_hi = range_lo + ranges;
+  count_scan_kernel<BINS><<<BINS / count_scan_nt<BINS>(), count_scan_nt<BINS>(), 0, s>>>(counts, n, range, starts,
+                                                                                          range_lo, range_hi);
   HPCS_CUDA(cudaGetLastError());
-  const int64_t range = int64_t(COUNT_FILL_NT) * COUNT_FILL_VPT * (16 / int64_t(sizeof(U)));
-  const int64_t fwant = (n + range - 1) / range;
-  const int fgrid = int(fwant > int64_t(ctx->sms) * 8 ? int64_t(ctx->sms) * 8 : fwant);
+  const int fgrid = int(ranges > int64_t(ctx->sms) * 8 ? int64_t(ctx->sms) * 8 : ranges);
   {
     KernelTimer kt(ctx, s, HPCS_K_FINALIZE);
-    count_fill_kernel<U><<<fgrid, COUNT_FILL_NT, 0, s>>>(d, n, starts, flip);
+    count_fill_kernel<U><<<fgrid, COUNT_FILL_NT, 0, s>>>(d, n, starts, range_lo, range_hi, flip);
     HPCS_CUDA(cudaGetLastError());
   }
   return HPCS_OK;

@@ -109,40 +109,66 @@ __global__ void __launch_bounds__(COUNT_NT) count_hist_kernel(const T* __restric
   }
 }
 
-// Exclusive scan of the counts into starts[0..BINS] (starts[BINS] = n), one CTA.
+// Exclusive scan of the counts into starts[0..BINS] (starts[BINS] = n), in CTAs of
+// count_scan_nt<BINS>() bins: CTA j adds up the counts of the bins before its chunk (coalesced
+// reads), then scans its own bins.  Each non-empty bin also records itself as the bin of every
+// fill range's first and last output that it holds (range r = outputs [r*R, min(n, (r+1)*R))):
+// range_lo[r] and range_hi[r], so the fill needs no search for its ranges' bounds.  A bin
+// spanning many ranges records them in a loop of its own thread.
 template <int BINS>
-__global__ void __launch_bounds__(COUNT_NT) count_scan_kernel(const uint32_t* __restrict__ counts,
-                                                              int64_t* __restrict__ starts) {
-  constexpr int PER = BINS / COUNT_NT > 0 ? BINS / COUNT_NT : 1;  // bins per thread
-  __shared__ int64_t s_w[COUNT_NT / 32];
+__host__ __device__ constexpr int count_scan_nt() {
+  return BINS < 1024 ? BINS : 1024;
+}
+
+template <int BINS>
+__global__ void __launch_bounds__(1024) count_scan_kernel(const uint32_t* __restrict__ counts, int64_t n, int64_t R,
+                                                          int64_t* __restrict__ starts, int32_t* __restrict__ range_lo,
+                                                          int32_t* __restrict__ range_hi) {
+  constexpr int NT = count_scan_nt<BINS>();
+  constexpr int NW = NT / 32;
+  __shared__ int64_t s_w[NW];
+  __shared__ int64_t s_base;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int b0 = tid * PER;
-  int64_t sum = 0;
-  for (int q = 0; q < PER; q++)
-    if (b0 + q < BINS) sum += counts[b0 + q];
-  int64_t incl = sum;
+  const int b0 = blockIdx.x * NT;
+  int64_t pre = 0;
+#pragma unroll 8
+  for (int i = tid; i < b0; i += NT) pre += counts[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) pre += __shfl_xor_sync(0xFFFFFFFFu, pre, o);
+  if (lane == 0) s_w[warp] = pre;
+  __syncthreads();
+  if (tid == 0) {
+    int64_t t = 0;
+    for (int w = 0; w < NW; w++) t += s_w[w];
+    s_base = t;
+  }
+  __syncthreads();
+  const int b = b0 + tid;
+  const int64_t c = counts[b];
+  int64_t incl = c;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const int64_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
     if (lane >= o) incl += y;
   }
+  __syncthreads();  // s_w is reused
   if (lane == 31) s_w[warp] = incl;
   __syncthreads();
-  int64_t base = 0;
-  for (int w = 0; w < warp; w++) base += s_w[w];
-  int64_t run = base + incl - sum;
-  for (int q = 0; q < PER; q++) {
-    if (b0 + q < BINS) {
-      starts[b0 + q] = run;
-      run += counts[b0 + q];
-    }
+  int64_t excl = s_base + incl - c;
+  for (int w = 0; w < warp; w++) excl += s_w[w];
+  starts[b] = excl;
+  if (b == BINS - 1) starts[BINS] = excl + c;
+  if (c > 0) {
+    const int64_t end = excl + c;  // this bin holds outputs [excl, end)
+    for (int64_t r = (excl + R - 1) / R; r * R < end; r++) range_lo[r] = b;
+    for (int64_t r = (excl + R) / R - 1; (r + 1) * R - 1 < end && (r + 1) * R - 1 < n; r++) range_hi[r] = b;
+    if (n - 1 >= excl && n - 1 < end) range_hi[(n - 1) / R] = b;  // the last range ends at n - 1
   }
-  if (tid == COUNT_NT - 1) starts[BINS] = base + incl;
 }
 
 // Fills out[i] with the value v whose run [starts[v], starts[v+1]) holds i.  Each CTA takes
-// ranges of COUNT_FILL_KEYS outputs (grid-stride): it finds the bins of the range's first and
-// last output by binary search over the starts, copies those bins' starts into shared memory
+// ranges of count_fill_range outputs (grid-stride): the scan recorded the bins of the range's
+// first and last output (range_lo, range_hi), and the CTA copies those bins' starts into shared memory
 // (when there are at most COUNT_FILL_SMEM of them; otherwise the searches below stay in
 // global memory), and each thread writes 16-byte vectors: the bin of a vector's first element
 // by binary search over the copied starts, then a walk across bin boundaries.  Unaligned
@@ -153,11 +179,19 @@ constexpr int COUNT_FILL_VPT = 16;  // vectors per thread and range
 constexpr int COUNT_FILL_SMEM = 2048;
 
 template <class T>
+__host__ __device__ constexpr int64_t count_fill_range() {
+  return int64_t(COUNT_FILL_NT) * COUNT_FILL_VPT * (16 / int64_t(sizeof(T)));
+}
+
+template <class T>
 __global__ void __launch_bounds__(COUNT_FILL_NT) count_fill_kernel(T* __restrict__ out, int64_t n,
-                                                                   const int64_t* __restrict__ starts, uint32_t flip) {
+                                                                   const int64_t* __restrict__ starts,
+                                                                   const int32_t* __restrict__ range_lo,
+                                                                   const int32_t* __restrict__ range_hi,
+                                                                   uint32_t flip) {
   constexpr int BINS = CountTraits<T>::BINS;
   constexpr int VEC = 16 / int(sizeof(T));
-  constexpr int64_t R = int64_t(COUNT_FILL_NT) * COUNT_FILL_VPT * VEC;  // outputs per range
+  constexpr int64_t R = count_fill_range<T>();  // outputs per range
   __shared__ int64_t s_st[COUNT_FILL_SMEM + 1];
   __shared__ int s_lo, s_cnt;
   auto bin_of_global = [&](int64_t i) {  // largest v with starts[v] <= i (runs may be empty)
@@ -174,7 +208,7 @@ __global__ void __launch_bounds__(COUNT_FILL_NT) count_fill_kernel(T* __restrict
   for (int64_t a = int64_t(blockIdx.x) * R; a < n; a += int64_t(gridDim.x) * R) {
     const int64_t e = a + R < n ? a + R : n;
     if (tid == 0) {
-      const int lo = bin_of_global(a), hi = bin_of_global(e - 1);
+      const int lo = range_lo[a / R], hi = range_hi[a / R];  // the bins of outputs a and e - 1
       s_lo = lo;
       s_cnt = hi - lo + 2;  // starts[lo .. hi + 1]
     }

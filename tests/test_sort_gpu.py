@@ -282,6 +282,17 @@ def test_counting_sort_8_16_bit(ctx, dt, n):
     assert np.array_equal(b, want)
 
 
+@pytest.mark.parametrize("dt", [np.uint8, np.int16])
+def test_counting_sort_one_value_and_two_runs(ctx, dt):
+    """Runs that span every fill range of the output: all keys equal, and two values only."""
+    n = 3_000_017
+    for a in (np.full(n, 5, dtype=dt), np.where(np.arange(n) % 3 == 0, dt(-1 if dt == np.int16 else 200), dt(4))):
+        want = np.sort(a, kind="stable")
+        b = a.copy()
+        algorithm.SortCountingInPlace(b)
+        assert np.array_equal(b, want)
+
+
 def test_counting_sort_device_unaligned(ctx):
     import torch
 
