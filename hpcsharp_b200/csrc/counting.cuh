@@ -245,6 +245,12 @@ __global__ void __launch_bounds__(COUNT_FILL_NT) count_fill_kernel(T* __restrict
         int v;
         int64_t next;
         find(first, v, next);
+        if (first + VEC <= next) {  // the whole vector is one value's run: the value replicated
+          const uint32_t val = uint32_t(v) ^ flip;
+          const uint32_t w = sizeof(T) == 1 ? (val & 0xFFu) * 0x01010101u : (val & 0xFFFFu) * 0x00010001u;
+          reinterpret_cast<uint4*>(out)[first / VEC] = make_uint4(w, w, w, w);
+          continue;
+        }
         union {
           uint4 u;
           T e[VEC];
