@@ -2,9 +2,9 @@
  * hpcs_gpu.h - C ABI of the B200 (sm_100a) LSD radix-sort library (libhpcs_gpu.so).
  *
  * This is the drop-in boundary for HPCsharp's radix-sort hot path.  A .NET caller binds
- * these functions with P/Invoke behind the same extension methods
- * the reference exposes; every entry point below names the reference method it replaces
- * (paths relative to the HPCsharp project root).
+ * these functions with P/Invoke behind the same extension methods the reference exposes;
+ * every entry point below names the reference method it replaces (paths relative to the
+ * HPCsharp project root).
  *
  * Conventions
  *   - Every function returns an hpcs_status; nothing aborts, exits or traps.  The text of
@@ -366,7 +366,9 @@ int hpcs_server_destroy(hpcs_server* server);
  *     first call before any stream capture.
  *   - All calls on a device share the one scratch array, which keeps the last call's
  *     contents (each call clears what must start at zero).  Calls that overlap on the GPU --
- *     from several streams or host threads at once -- race and corrupt each other. */
+ *     from several streams or host threads at once -- race and corrupt each other.
+ *   - The set-up result is kept for the life of the process: a device reset
+ *     (cudaDeviceReset) between calls is not supported. */
 #define HPCS_NOALLOC_MAX_KEYS ((int64_t)1048576) /* 2^20 keys */
 int hpcs_sort_u32_dev_noalloc(uint32_t* keys, int64_t n, void* stream);
 

@@ -56,6 +56,12 @@ def lib():
         for t in ("u32", "i32", "u64", "i64"):
             getattr(L, f"orc_std_sort_{t}").argtypes = [P, I64]
         L.orc_hardware_threads.restype = I
+        L.orc_radix_par_ws_create.argtypes = [I64, I64, I]
+        L.orc_radix_par_ws_create.restype = P
+        L.orc_radix_par_ws_destroy.argtypes = [P]
+        L.orc_sort_radix_par_ws_k32.argtypes = [P, P, I64, I, I]
+        L.orc_sort_radix_par_ws_k64.argtypes = [P, P, I64, I, I]
+        L.orc_gen_u32_uniform.argtypes = [P, I64, C.c_uint64, I]
         _lib = L
     return _lib
 
@@ -86,6 +92,48 @@ def sort_radix_par(a: np.ndarray, threads: int = 0, quantum: int = 64 * 1024) ->
         getattr(L, f"orc_sort_radix_par_{t}")(a.ctypes.data, a.size, quantum, th)
     else:
         getattr(L, f"orc_sort_radix_par_{t}")(a.ctypes.data, a.size, th)
+    return a
+
+
+class RadixParWorkspace:
+    """Scratch of SortRadixPar made once: the output array and the per-quantum buffers, counts
+    and starts that the reference allocates at the top of each call (RadixSortLsdParallel.cs:
+    151-170).  sort() then runs the fully parallel restatement without allocating, so a timed
+    loop measures the sort alone."""
+
+    def __init__(self, n: int, itemsize: int = 4, quantum: int = 64 * 1024):
+        self.n, self.itemsize = int(n), int(itemsize)
+        self.handle = lib().orc_radix_par_ws_create(self.n, quantum, self.itemsize)
+        if not self.handle:
+            raise MemoryError("workspace creation failed")
+
+    def sort(self, a: np.ndarray, threads: int = 0) -> np.ndarray:
+        """Fully parallel SortRadixPar of a (any of the six key types) in place."""
+        if a.dtype.itemsize != self.itemsize or a.size > self.n or not a.flags.c_contiguous:
+            raise ValueError("array does not fit the workspace")
+        th = threads if threads > 0 else hardware_threads()
+        fn = lib().orc_sort_radix_par_ws_k32 if self.itemsize == 4 else lib().orc_sort_radix_par_ws_k64
+        if fn(self.handle, a.ctypes.data, a.size, KIND[_name(a)], th) != 0:
+            raise RuntimeError("SortRadixPar workspace call failed")
+        return a
+
+    def close(self) -> None:
+        if self.handle:
+            lib().orc_radix_par_ws_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gen_u32_uniform(n: int, seed: int = 1, threads: int = 0) -> np.ndarray:
+    """The benchmark's uniform uint32 keys (PCG32 per 64 Ki chunk), generated here so that a CPU
+    baseline loads no library of the product; equal to hpcsharp_b200.datagen.u32_uniform."""
+    a = np.empty(int(n), dtype=np.uint32)
+    lib().orc_gen_u32_uniform(a.ctypes.data, a.size, seed, threads if threads > 0 else hardware_threads())
     return a
 
 

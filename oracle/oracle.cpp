@@ -175,21 +175,39 @@ void histogram_byte_components_par(const U* a, int64_t l, int64_t r, int kind, u
 //   one task per quantum runs SortRadixDeRandomizedInnerFunction (:96-135): scatter through
 //     64-deep per-bin buffers, flush when full, final flush;
 //   Task.WaitAll, swap buffers (:216-225).
+// Scratch of one SortRadixPar call: the output array and, per work quantum, the 256 x 64-key
+// de-randomisation buffers, the bin counts and the bin starts.  The reference allocates all of
+// them once per call before its digit loop (RadixSortLsdParallel.cs:151-170); a caller that
+// times repeated sorts allocates them once outside the timed region (RadixParWorkspace below).
 template <class U>
-void sort_radix_par_full(U* a, int64_t n, int kind, int64_t quantum, int threads) {
+struct RadixParScratch {
+  U* out;            // n keys
+  U* buffers;        // quanta x 256 x 64 keys
+  uint32_t* count;   // quanta x 256
+  int64_t* start;    // quanta x 256
+};
+
+// Fully parallel u32 LSD: SortRadixPar(uint[], ParallelWorkQuantum = 64 Ki)
+// RadixSortLsdParallel.cs:145-232.  Per digit pass:
+//   ComputeStartOfBinsPar (:49-94): per-quantum histogram of this digit
+//     (HistogramByteComponentsAcrossWorkQuantasQC, Histogram.cs:574-637), then start offsets
+//     ordered bin-major, quantum-minor (stable);
+//   one task per quantum runs SortRadixDeRandomizedInnerFunction (:96-135): scatter through
+//     64-deep per-bin buffers (one set per quantum, :159-161), flush when full, final flush;
+//   Task.WaitAll, swap buffers (:216-225).
+template <class U>
+void sort_radix_par_full_ws(U* a, int64_t n, int kind, int64_t quantum, int threads, const RadixParScratch<U>& ws) {
   constexpr int P = sizeof(U);
   if (n <= 0) return;
-  if (quantum <= 0) quantum = 64 * 1024;
   const int64_t quanta = (n + quantum - 1) / quantum;
   const int64_t depth = 64;  // BufferDepth (:158)
-  std::vector<U> outv(n);
   U* in = a;
-  U* out = outv.data();
-  std::vector<uint32_t> count(size_t(quanta) * 256);
-  std::vector<int64_t> start(size_t(quanta) * 256);
+  U* out = ws.out;
+  uint32_t* count = ws.count;
+  int64_t* start = ws.start;
   for (int d = 0; d < P; d++) {
     parallel_for(quanta, threads, [&](int64_t q) {
-      uint32_t* c = count.data() + q * 256;
+      uint32_t* c = count + q * 256;
       std::memset(c, 0, 256 * sizeof(uint32_t));
       int64_t lo = q * quantum, hi = std::min(n, lo + quantum);
       for (int64_t i = lo; i < hi; i++) c[digit_of<U>(in[i], d, kind)]++;
@@ -202,9 +220,9 @@ void sort_radix_par_full(U* a, int64_t n, int kind, int64_t quantum, int threads
         run += count[q * 256 + b];
       }
     parallel_for(quanta, threads, [&](int64_t q) {
-      std::vector<U> buf(256 * depth);
+      U* buf = ws.buffers + q * 256 * depth;
       int64_t idx[256];
-      int64_t* sob = start.data() + q * 256;
+      int64_t* sob = start + q * 256;
       for (int b = 0; b < 256; b++) idx[b] = b * depth;
       int64_t lo = q * quantum, hi = std::min(n, lo + quantum);
       for (int64_t i = lo; i < hi; i++) {
@@ -212,7 +230,7 @@ void sort_radix_par_full(U* a, int64_t n, int kind, int64_t quantum, int threads
         if (idx[b] < int64_t(b) * depth + depth) {
           buf[idx[b]++] = in[i];
         } else {
-          std::memcpy(out + sob[b], buf.data() + b * depth, sizeof(U) * depth);
+          std::memcpy(out + sob[b], buf + b * depth, sizeof(U) * depth);
           sob[b] += depth;
           buf[b * depth] = in[i];
           idx[b] = b * depth + 1;
@@ -220,13 +238,40 @@ void sort_radix_par_full(U* a, int64_t n, int kind, int64_t quantum, int threads
       }
       for (int b = 0; b < 256; b++) {
         int64_t items = idx[b] - int64_t(b) * depth;
-        std::memcpy(out + sob[b], buf.data() + b * depth, sizeof(U) * items);
+        std::memcpy(out + sob[b], buf + b * depth, sizeof(U) * items);
         sob[b] += items;
       }
     });
     std::swap(in, out);
   }
   if (in != a) std::memcpy(a, in, sizeof(U) * n);
+}
+
+// Owns the scratch of sort_radix_par_full_ws for arrays of up to n keys.
+struct RadixParWorkspace {
+  int64_t n = 0, quantum = 0, width = 0;
+  std::vector<unsigned char> out, buffers;
+  std::vector<uint32_t> count;
+  std::vector<int64_t> start;
+  RadixParWorkspace(int64_t n_, int64_t quantum_, int64_t width_) : n(n_), quantum(quantum_), width(width_) {
+    const int64_t quanta = (n + quantum - 1) / quantum;
+    out.resize(size_t(n * width));
+    buffers.resize(size_t(quanta * 256 * 64 * width));
+    count.resize(size_t(quanta * 256));
+    start.resize(size_t(quanta * 256));
+  }
+  template <class U>
+  RadixParScratch<U> scratch() {
+    return {reinterpret_cast<U*>(out.data()), reinterpret_cast<U*>(buffers.data()), count.data(), start.data()};
+  }
+};
+
+template <class U>
+void sort_radix_par_full(U* a, int64_t n, int kind, int64_t quantum, int threads) {
+  if (n <= 0) return;
+  if (quantum <= 0) quantum = 64 * 1024;
+  RadixParWorkspace ws(n, quantum, int64_t(sizeof(U)));
+  sort_radix_par_full_ws<U>(a, n, kind, quantum, threads, ws.scratch<U>());
 }
 
 // Partially parallel LSD: SortRadixPar(int[]) :446-495, (long[]) :560-609, (ulong[])
@@ -437,6 +482,52 @@ void orc_sort_radix_lsd_f64(double* a, int64_t n) {
 // Parallel SortRadixPar: fully parallel for u32 (:145-232); partially parallel for i32/u64/i64
 // (:446-734); f32/f64 use the fully parallel structure with the float transform (the
 // reference has no float LSD; the transform is Histogram.cs:1210-1288).
+// SortRadixPar on a workspace made once (orc_radix_par_ws_create) for arrays of up to its n
+// keys of `width` bytes: the timed CPU baseline allocates nothing inside the sort.
+void* orc_radix_par_ws_create(int64_t n, int64_t quantum, int width) {
+  if (n < 0 || (width != 4 && width != 8)) return nullptr;
+  if (quantum <= 0) quantum = 64 * 1024;
+  return new RadixParWorkspace(n, quantum, width);
+}
+void orc_radix_par_ws_destroy(void* ws) { delete static_cast<RadixParWorkspace*>(ws); }
+int orc_sort_radix_par_ws_k32(void* wsp, uint32_t* a, int64_t n, int kind, int threads) {
+  auto* ws = static_cast<RadixParWorkspace*>(wsp);
+  if (!ws || ws->width != 4 || n > ws->n) return 1;
+  sort_radix_par_full_ws<uint32_t>(a, n, kind, ws->quantum, threads, ws->scratch<uint32_t>());
+  return 0;
+}
+int orc_sort_radix_par_ws_k64(void* wsp, uint64_t* a, int64_t n, int kind, int threads) {
+  auto* ws = static_cast<RadixParWorkspace*>(wsp);
+  if (!ws || ws->width != 8 || n > ws->n) return 1;
+  sort_radix_par_full_ws<uint64_t>(a, n, kind, ws->quantum, threads, ws->scratch<uint64_t>());
+  return 0;
+}
+
+// The benchmark's uniform uint32 keys, restated so that the CPU baseline needs no library of
+// the product: element i belongs to chunk c = i / 65536 and chunk c draws from PCG32 (O'Neill's
+// published minimal generator, pcg-random.org) seeded with (initstate = seed, initseq = c).
+// tests/test_oracle.py checks it against the generator the GPU workloads use.
+void orc_gen_u32_uniform(uint32_t* out, int64_t n, uint64_t seed, int threads) {
+  const int64_t chunk = 65536;
+  const int64_t chunks = (n + chunk - 1) / chunk;
+  parallel_for(chunks, threads, [&](int64_t c) {
+    uint64_t inc = (uint64_t(c) << 1u) | 1u;
+    uint64_t state = 0u;
+    auto step = [&]() {
+      uint64_t old = state;
+      state = old * 6364136223846793005ULL + inc;
+      uint32_t xs = uint32_t(((old >> 18u) ^ old) >> 27u);
+      uint32_t rot = uint32_t(old >> 59u);
+      return (xs >> rot) | (xs << ((32u - rot) & 31u));
+    };
+    step();
+    state += seed;
+    step();
+    const int64_t lo = c * chunk, hi = std::min(n, lo + chunk);
+    for (int64_t i = lo; i < hi; i++) out[i] = step();
+  });
+}
+
 void orc_sort_radix_par_u32(uint32_t* a, int64_t n, int64_t quantum, int threads) {
   sort_radix_par_full<uint32_t>(a, n, UNSIGNED, quantum, threads);
 }

@@ -1,15 +1,29 @@
-"""Full-size workloads (the plain-sort-at-scale and pairs configurations) checked through
+"""Full-size workloads (the plain-sort-at-scale and pairs configurations): 256 Mi u32 uniform,
+i32 normal(0, 2^20) and f32 normal(0,1) with specials; 128 Mi u64 uniform and AND-of-3;
+200 M u64 Zipf(1.1) keys + u32 index items; 100 M f64 normal(0,1) keys + index items.
+
+Each output is compared byte for byte with the oracle's SortRadixPar / SortRadix<T>(items,
+keys) restatement run on the same seeded input on the host cores, and also checked through
 size-independent properties on the GPU: the output is in the reference's key order, it is a
 permutation of the input (order-independent checksums), and for key+index pairs every item
-points at its key in the input and equal keys keep their input order (stability).  The
-bit-exact oracle comparisons run at smaller sizes in the other test files."""
+points at its key in the input and equal keys keep their input order (stability)."""
 import numpy as np
 import pytest
 
 from hpcsharp_b200 import datagen, native
-from tests.gpu_util import checksum_dev, is_sorted_dev, ordered_i64, to_dev
+from tests.gpu_util import checksum_dev, from_dev, is_sorted_dev, ordered_i64, to_dev
 
 pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+
+def assert_same_bytes(got: np.ndarray, want: np.ndarray) -> None:
+    assert got.shape == want.shape and got.dtype.itemsize == want.dtype.itemsize
+    gu = got.view(np.uint32 if got.dtype.itemsize == 4 else np.uint64)
+    wu = want.view(gu.dtype)
+    if not np.array_equal(gu, wu):
+        bad = np.flatnonzero(gu != wu)
+        raise AssertionError(f"{bad.size} keys differ from the oracle, first at {bad[:5]}")
+
 
 PLAIN = [
     ("u32", 1 << 28, lambda n: datagen.u32_uniform(n, 1)),
@@ -22,7 +36,7 @@ PLAIN = [
 
 @pytest.mark.parametrize("dt,n,gen", PLAIN, ids=["u32_256M", "i32_normal_256M", "f32_specials_256M",
                                                  "u64_uniform_128M", "u64_and3_128M"])
-def test_plain_sort_at_scale(ctx, dt, n, gen):
+def test_plain_sort_at_scale(ctx, orc, dt, n, gen):
     import torch
 
     a = gen(n)
@@ -33,8 +47,11 @@ def test_plain_sort_at_scale(ctx, dt, n, gen):
     ctx.synchronize()
     assert is_sorted_dev(t, dt)
     assert checksum_dev(t) == before
+    got = from_dev(t, a.dtype)
     del t
     torch.cuda.empty_cache()
+    orc.sort_radix_par(a)  # in place: now the reference's result
+    assert_same_bytes(got, a)
 
 
 PAIRS = [
@@ -44,7 +61,7 @@ PAIRS = [
 
 
 @pytest.mark.parametrize("dt,n,gen", PAIRS, ids=["u64_zipf_200M_pairs", "f64_normal_100M_pairs"])
-def test_pairs_at_scale(ctx, dt, n, gen):
+def test_pairs_at_scale(ctx, orc, dt, n, gen):
     import torch
 
     a = gen(n)
@@ -66,8 +83,14 @@ def test_pairs_at_scale(ctx, dt, n, gen):
     assert bool((idx[1:][same] > idx[:-1][same]).all())
     if dt == "u64":
         assert int(same.sum()) > n // 2  # Zipf duplicates are heavy
+    got_keys = from_dev(keys, a.dtype)
+    got_items = from_dev(items, np.uint32)
     del keys, orig, items, idx, o, same
     torch.cuda.empty_cache()
+    want_items = np.arange(n, dtype=np.uint32)
+    orc.sort_pairs(a, want_items)  # in place: the reference's keys and stable permutation
+    assert_same_bytes(got_keys, a)
+    assert_same_bytes(got_items, want_items)
 
 
 def test_sort_beyond_2_to_30_keys(ctx):

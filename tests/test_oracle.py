@@ -148,3 +148,33 @@ def test_select_topk_duplicates(orc):
         assert orc.select_topk(b, k) == 0
         assert b[k] == srt[k]
         np.testing.assert_array_equal(np.sort(b[k:]), srt[k:])
+
+
+@pytest.mark.parametrize("n", [0, 1, 65535, 65536, 65537, 3_000_017])
+def test_oracle_key_stream_equals_product_generator(orc, n):
+    """The CPU baseline generates its keys inside the oracle; they must be the very keys the GPU
+    benchmark sorts (same SHA-256), so both arms run the same configuration."""
+    import hashlib
+
+    a = orc.gen_u32_uniform(n, seed=1, threads=3)
+    b = datagen.u32_uniform(n, 1)
+    assert hashlib.sha256(a.tobytes()).hexdigest() == hashlib.sha256(b.tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("dt", ["u32", "i32", "f32", "u64", "i64", "f64"])
+def test_workspace_sort_radix_par_equals_serial(orc, dt):
+    """SortRadixPar on a workspace made once (scratch allocated outside the sort) gives the
+    serial restatement's result, on two calls in a row of different sizes."""
+    ws = orc.RadixParWorkspace(400_000, np.dtype(datagen.by_name(dt, 1).dtype).itemsize)
+    try:
+        for n, seed in ((400_000, 3), (123_457, 4)):
+            a = datagen.by_name(dt, n, seed=seed)
+            s = a.copy()
+            orc.sort_radix_lsd(s)
+            w = a.copy()
+            ws.sort(w, threads=3)
+            np.testing.assert_array_equal(w.view(np.uint8), s.view(np.uint8))
+        with pytest.raises(ValueError):
+            ws.sort(datagen.by_name(dt, 400_001, seed=1))
+    finally:
+        ws.close()

@@ -27,16 +27,32 @@ def _entry():
     return lib, fn
 
 
-def test_no_alloc_sort_matches_context_sort_twice():
+def _inputs(kind: str, n: int, seed: int) -> np.ndarray:
+    a = datagen.u32_uniform(n, seed=seed)
+    if kind == "below_2_24":
+        return a & np.uint32(0x00FFFFFF)  # top digit all zero: three passes run, an odd number
+    if kind == "constant":
+        return np.full(n, 0xDEADBEEF, dtype=np.uint32)  # every pass skipped
+    return a
+
+
+# (keys, n, seed) of consecutive calls: the scratch keeps each call's contents for the next
+CALLS = [("uniform", NOALLOC_MAX_KEYS, 101), ("uniform", 777_777, 202), ("below_2_24", 999_999, 303),
+         ("constant", 65_537, 404), ("uniform", 4_099, 505)]
+
+
+def test_no_alloc_sort_matches_context_sort_and_numpy():
+    """Several calls in a row, each compared bit for bit with the context-based sort and with
+    numpy's sort: whole digit passes, an odd number of executed passes (the result comes back
+    from the scratch array) and all passes skipped."""
     import torch
 
     lib, fn = _entry()
     ctx = native.Context(0)
     try:
         stream = torch.cuda.current_stream().cuda_stream
-        # two calls in a row, the second smaller (the scratch keeps the first call's contents)
-        for n, seed in ((NOALLOC_MAX_KEYS, 101), (777_777, 202)):
-            a = datagen.u32_uniform(n, seed=seed)
+        for kind, n, seed in CALLS:
+            a = _inputs(kind, n, seed)
             t_noalloc = to_dev(a)
             t_regular = to_dev(a)
             rc = fn(t_noalloc.data_ptr(), n, stream)
@@ -45,9 +61,8 @@ def test_no_alloc_sort_matches_context_sort_twice():
             torch.cuda.synchronize()
             ctx.synchronize()
             got = from_dev(t_noalloc, np.uint32)
-            want = from_dev(t_regular, np.uint32)
-            np.testing.assert_array_equal(got, want)
-            assert np.all(got[1:] >= got[:-1])
+            np.testing.assert_array_equal(got, from_dev(t_regular, np.uint32))
+            np.testing.assert_array_equal(got, np.sort(a))
     finally:
         ctx.close()
 
