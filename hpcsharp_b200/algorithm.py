@@ -19,6 +19,10 @@ Reference surface (paths relative to the HPCsharp project root):
   ParallelAlgorithm.SortCounting[InPlace[Func]]Par(...)                   CountingSortParallel.cs:22-99
   Algorithm.SelectRadix(this uint[]/ulong[], k or int[] k [, start, length])
                                                                        SelectionRadix.cs:236-435
+  ParallelAlgorithm.SelectRadixPar(this uint[], [start, length,] k, parallelThreshold)
+                                                                       SelectionRadixParallel.cs:254-283
+  Algorithm.PartitionRadix(this uint[]/ulong[], [start, length,] k or int[] k, threshold)
+                                                                       PartitionRadix.cs:135-210
 
 Arrays are numpy arrays sorted in place (the reference's SortRadixPar returns the caller's
 array after an even number of passes, RadixSortLsdParallel.cs:227-231).  float32/float64
@@ -146,38 +150,72 @@ def SelectTopK(arrayToBeSelected: np.ndarray, *args) -> None:
     default_context().select_topk(a[start:start + length], k - start)
 
 
+def _select_args(a, args, what: str):
+    """(start, length, k) from the reference's overloads (k or (start, length, k))."""
+    if len(args) == 1:
+        if a.size <= 0:
+            raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "array length is invalid")
+        return 0, a.size, args[0]
+    if len(args) == 3:
+        start, length, k = args
+        if start < 0 or length <= 0 or start + length > a.size:
+            raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "array length or length is invalid")
+        return int(start), int(length), k
+    raise TypeError(f"{what}: expected (k) or (start, length, k)")
+
+
 def SelectRadix(arrayToBeSelected: np.ndarray, *args):
     """SelectRadix (SelectionRadix.cs:236-435), in place, on the GPU's radix select:
-      SelectRadix(a, k) / SelectRadix(a, start, length, k) -> the k-th smallest key (0-based;
-        k indexes the whole array), left at a[k] with a[k..] holding the larger keys;
+      SelectRadix(a, k) / SelectRadix(a, start, length, k) -> the k-th smallest key of the
+        (sub)array (k indexes the whole array), left at a[k] with the (sub)array partitioned
+        around it;
       SelectRadix(a, k_list) / SelectRadix(a, start, length, k_list) -> None; afterwards every
-        a[k_i] holds the k_i-th smallest key of the (sub)array.  The several-k form sorts the
-        (sub)array, which satisfies every k at once."""
+        a[k_i] holds the key the sorted (sub)array has at k_i (PartitionRadix by every k)."""
     _require(arrayToBeSelected, "arrayToBeSelected")
     a = arrayToBeSelected
-    if len(args) in (1, 3) and np.ndim(args[-1]) == 1:
-        ks = [int(x) for x in args[-1]]
-        start, length = (0, a.size) if len(args) == 1 else (int(args[0]), int(args[1]))
-        if start < 0 or length <= 0 or start + length > a.size:
-            raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "l or r are invalid")
-        for k in ks:
-            if k < start or k >= start + length:
-                raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "k must be between start and (start + length)")
-        default_context().sort(a[start:start + length])
+    start, length, k = _select_args(a, args, "SelectRadix")
+    if np.ndim(k) == 1:
+        PartitionRadix(a, start, length, k)
         return None
-    if len(args) == 1:
-        k = int(args[0])
-        if a.size <= 0 or k < 0 or k >= a.size:
-            raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "k must be between start and (start + length)")
-        default_context().select_topk(a, k)
-        return a[k]
-    start, length, k = (int(x) for x in args)
-    if start < 0 or length <= 0 or start + length > a.size:
-        raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "l or r are invalid")
+    k = int(k)
     if k < start or k >= start + length:
         raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "k must be between start and (start + length)")
-    default_context().select_topk(a[start:start + length], k - start)
-    return a[k]
+    return default_context().select_radix(a, start, length, k)
+
+
+def SelectRadixPar(arrayToBeSelected: np.ndarray, *args, parallelThreshold: int = 64 * 1024):
+    """SelectRadixPar(a, k) / (a, start, length, k) (SelectionRadixParallel.cs:254-283): the k-th
+    smallest key of the (sub)array, k indexing the whole array; it is also left at a[k].  The
+    parallel threshold is the reference's CPU task size and has no effect on the GPU."""
+    _require(arrayToBeSelected, "arrayToBeSelected")
+    a = arrayToBeSelected
+    start, length, k = _select_args(a, args, "SelectRadixPar")
+    k = int(k)
+    if k < start or k >= start + length:
+        raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "k must be between start and (start + length)")
+    return default_context().select_radix(a, start, length, k)
+
+
+def PartitionRadix(arrayToBePartitioned: np.ndarray, *args, threshold: int = 1024) -> None:
+    """PartitionRadix(a, k | k[]) / (a, start, length, k | k[]) (PartitionRadix.cs:135-210), in
+    place: afterwards every a[k_i] holds the key the sorted (sub)array has at k_i and the keys
+    between two consecutive indices lie between their keys (nth_element).  k indexes the whole
+    array.  The base-case threshold is the reference's CPU knob and has no effect on the GPU."""
+    _require(arrayToBePartitioned, "arrayToBePartitioned")
+    a = arrayToBePartitioned
+    start, length, k = _select_args(a, args, "PartitionRadix")
+    if k is None:
+        raise ArgumentNullException(HPCS_ERR_NULL, "k is null")
+    ks = np.atleast_1d(np.asarray(k, dtype=np.int64))
+    if ks.size > a.size:
+        raise ArgumentOutOfRangeException(HPCS_ERR_RANGE,
+                                          "k array length cannot be greater than the array to be selected length")
+    if ks.size == 0:
+        return None
+    if ((ks < start) | (ks >= start + length)).any():
+        raise ArgumentOutOfRangeException(HPCS_ERR_RANGE, "k must be between start and (start + length)")
+    default_context().partition_radix(a, start, length, ks)
+    return None
 
 
 def SortRadixMsd(arrayToBeSorted: np.ndarray) -> np.ndarray:

@@ -20,10 +20,11 @@ CSRC = os.path.join(PKG, "csrc")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
     "-Xptxas", "-warn-spills",
     "--expt-relaxed-constexpr",
 ]
+OBJ_DIR = os.path.join(ROOT, "_build")
 
 GPU_SOURCES = ["capi.cu", "noalloc.cu", "segmented_host.cu", "serve.cu"]
 
@@ -63,12 +64,20 @@ def build_gpu(force: bool = False, verbose_ptxas: bool = False, out: str | None 
     srcs = [os.path.join(CSRC, s) for s in GPU_SOURCES]
     deps = srcs + _gpu_deps() + [os.path.join(ROOT, "include", "hpcs_gpu.h")]
     if force or _stale(out, deps):
+        from concurrent.futures import ThreadPoolExecutor
+
         flags = list(NVCC_FLAGS)
         if verbose_ptxas:
             flags += ["-Xptxas", "-v"]
         for d in defines or []:
             flags += ["-D" + d]
-        _run([_nvcc(), *flags, "-o", out, *srcs])
+        # one object per translation unit, compiled concurrently, then one link
+        tag = os.path.splitext(os.path.basename(out))[0]
+        os.makedirs(OBJ_DIR, exist_ok=True)
+        objs = [os.path.join(OBJ_DIR, f"{tag}.{os.path.splitext(os.path.basename(src))[0]}.o") for src in srcs]
+        with ThreadPoolExecutor(max_workers=len(srcs)) as pool:
+            list(pool.map(lambda so: _run([_nvcc(), *flags, "-c", "-o", so[1], so[0]]), zip(srcs, objs)))
+        _run([_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", out, *objs])
     return out
 
 

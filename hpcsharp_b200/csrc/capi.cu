@@ -2,8 +2,11 @@
 // mirror the reference's exceptions, host-array and device-pointer entry points.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstddef>
 #include <cstdio>
 #include <string>
+#include <vector>
 
 #include "../../include/hpcs_gpu.h"
 #include "sort_host.cuh"
@@ -379,6 +382,85 @@ int select_topk_dev(hpcs_ctx* ctx, T* a, int64_t n, int64_t k, void* stream) {
   if ((rc = enqueue_select<U, KIND>(ctx, d, n, k, s, &st)) != HPCS_OK) return rc;
   if ((rc = enqueue_partition<U, KIND>(ctx, d, n, st, o, s)) != HPCS_OK) return rc;
   HPCS_CUDA(cudaMemcpyAsync(d, o, size_t(n) * sizeof(U), cudaMemcpyDeviceToDevice, s));
+  return HPCS_OK;
+}
+
+// ---- PartitionRadix / SelectRadix(Par) ---------------------------------------------------
+// Up to this many distinct k indices are placed by successive radix selects and three-way
+// partitions of the part above the previous one; more indices sort the subarray, which places
+// every index at once (a sorted array is a valid partition for any k).
+constexpr int64_t PARTITION_MAX_SELECTS = 4;
+static_assert(offsetof(SelectState, eq) == offsetof(SelectState, less) + sizeof(int64_t), "less, eq adjacent");
+
+int check_partition_args(hpcs_ctx* ctx, const void* a, int64_t start, int64_t length, const int64_t* ks,
+                         int64_t nk) {
+  if (!ctx) return fail(HPCS_ERR_NULL, "ctx is NULL");
+  if (!a) return fail(HPCS_ERR_NULL, "array is NULL");
+  if (nk > 0 && !ks) return fail(HPCS_ERR_NULL, "k is NULL");
+  // PartitionRadix.cs:139-140, :173-174; SelectionRadixParallel.cs:258-261
+  if (start < 0 || length <= 0) return fail(HPCS_ERR_RANGE, "array length or length is invalid");
+  if (length > HPCS_MAX_SEGMENT_KEYS) return fail(HPCS_ERR_RANGE, "length exceeds HPCS_MAX_SEGMENT_KEYS");
+  if (nk < 0) return fail(HPCS_ERR_RANGE, "the number of k indices is negative");
+  for (int64_t i = 0; i < nk; i++)
+    if (ks[i] < start || ks[i] >= start + length)
+      return fail(HPCS_ERR_RANGE, "k must be between start and (start + length)");
+  return HPCS_OK;
+}
+
+// Places the (ascending, distinct) relative ranks r[] in d[0..n) on the device: afterwards d[r_i]
+// is the key the sorted range has at r_i, and the keys between two consecutive r's lie between
+// their values.  o is scratch of n keys.  Successive selects and three-way partitions of the part
+// above the previous rank's run of equal keys, or one sort when there are many ranks.
+template <class U, int KIND>
+int enqueue_partition_ranks(hpcs_ctx* ctx, U* d, U* o, int64_t n, const std::vector<int64_t>& r, cudaStream_t s) {
+  int rc;
+  if (int64_t(r.size()) > PARTITION_MAX_SELECTS) return enqueue_sort<U, KIND, NoValue>(ctx, d, nullptr, n, s);
+  int64_t lo = 0;  // keys below lo are placed: every later rank lies at or above it
+  for (int64_t rank : r) {
+    if (rank < lo) continue;  // inside the previous rank's run of keys equal to its key
+    SelectState* st = nullptr;
+    if ((rc = enqueue_select<U, KIND>(ctx, d + lo, n - lo, rank - lo, s, &st)) != HPCS_OK) return rc;
+    if ((rc = enqueue_partition<U, KIND>(ctx, d + lo, n - lo, st, o + lo, s)) != HPCS_OK) return rc;
+    HPCS_CUDA(cudaMemcpyAsync(d + lo, o + lo, size_t(n - lo) * sizeof(U), cudaMemcpyDeviceToDevice, s));
+    int64_t less_eq[2] = {0, 0};  // SelectState::less and ::eq are adjacent
+    HPCS_CUDA(cudaMemcpyAsync(less_eq, &st->less, sizeof(less_eq), cudaMemcpyDeviceToHost, s));
+    HPCS_CUDA(cudaStreamSynchronize(s));
+    lo += less_eq[0] + less_eq[1];
+  }
+  return HPCS_OK;
+}
+
+// PartitionRadix(this T[] a, int start, int length, int k / int[] k): host array, in place.
+template <class T, class U, int KIND>
+int partition_radix_host(hpcs_ctx* ctx, T* a, int64_t start, int64_t length, const int64_t* ks, int64_t nk) {
+  int rc = check_partition_args(ctx, a, start, length, ks, nk);
+  if (rc != HPCS_OK || nk == 0) return rc;
+  std::vector<int64_t> r(ks, ks + nk);
+  for (auto& x : r) x -= start;
+  std::sort(r.begin(), r.end());
+  r.erase(std::unique(r.begin(), r.end()), r.end());
+  DeviceGuard g(ctx->device);
+  cudaStream_t s = ctx->stream;
+  if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->keys_a, size_t(length) * sizeof(U))) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->vals_a, size_t(length) * sizeof(U))) != HPCS_OK) return rc;
+  U* d = static_cast<U*>(ctx->keys_a.ptr);
+  U* o = static_cast<U*>(ctx->vals_a.ptr);
+  HPCS_CUDA(cudaMemcpyAsync(d, a + start, size_t(length) * sizeof(U), cudaMemcpyHostToDevice, s));
+  if ((rc = enqueue_partition_ranks<U, KIND>(ctx, d, o, length, r, s)) != HPCS_OK) return rc;
+  HPCS_CUDA(cudaMemcpyAsync(a + start, d, size_t(length) * sizeof(U), cudaMemcpyDeviceToHost, s));
+  HPCS_CUDA(cudaStreamSynchronize(s));
+  return check_device_errors(ctx);
+}
+
+// SelectRadix / SelectRadixPar(this T[] a, int start, int length, int k): the k-th smallest key of
+// a[start, start + length) (k absolute) into *out, left at a[k]; a is partitioned around it.
+template <class T, class U, int KIND>
+int select_radix_host(hpcs_ctx* ctx, T* a, int64_t start, int64_t length, int64_t k, T* out) {
+  if (!out) return fail(HPCS_ERR_NULL, "out is NULL");
+  int rc = partition_radix_host<T, U, KIND>(ctx, a, start, length, &k, 1);
+  if (rc != HPCS_OK) return rc;
+  *out = a[k];
   return HPCS_OK;
 }
 
@@ -770,6 +852,21 @@ HPCS_TOPK_EXPORTS(f32, float, uint32_t, KIND_FLOAT)
 HPCS_TOPK_EXPORTS(u64, uint64_t, uint64_t, KIND_UNSIGNED)
 HPCS_TOPK_EXPORTS(i64, int64_t, uint64_t, KIND_SIGNED)
 HPCS_TOPK_EXPORTS(f64, double, uint64_t, KIND_FLOAT)
+
+#define HPCS_PARTITION_EXPORTS(NAME, T, U, KIND)                                                      \
+  int hpcs_partition_radix_##NAME(hpcs_ctx* c, T* a, int64_t start, int64_t length, const int64_t* k,     \
+                                  int64_t nk) {                                                            \
+    return partition_radix_host<T, U, KIND>(c, a, start, length, k, nk);                                   \
+  }                                                                                                        \
+  int hpcs_select_radix_##NAME(hpcs_ctx* c, T* a, int64_t start, int64_t length, int64_t k, T* out) {     \
+    return select_radix_host<T, U, KIND>(c, a, start, length, k, out);                                     \
+  }
+HPCS_PARTITION_EXPORTS(u32, uint32_t, uint32_t, KIND_UNSIGNED)
+HPCS_PARTITION_EXPORTS(i32, int32_t, uint32_t, KIND_SIGNED)
+HPCS_PARTITION_EXPORTS(f32, float, uint32_t, KIND_FLOAT)
+HPCS_PARTITION_EXPORTS(u64, uint64_t, uint64_t, KIND_UNSIGNED)
+HPCS_PARTITION_EXPORTS(i64, int64_t, uint64_t, KIND_SIGNED)
+HPCS_PARTITION_EXPORTS(f64, double, uint64_t, KIND_FLOAT)
 
 int hpcs_histogram_byte_components_dev(hpcs_ctx* ctx, int dtype, const void* a, int64_t n, uint32_t* counts,
                                        void* stream) {

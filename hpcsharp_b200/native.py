@@ -155,6 +155,8 @@ def _declare(lib) -> None:
         getattr(lib, f"hpcs_select_topk_{t}_dev").argtypes = [P, P, I64, I64, P]
         getattr(lib, f"hpcs_topk_largest_{t}").argtypes = [P, P, I64, I64, P]
         getattr(lib, f"hpcs_topk_largest_{t}_dev").argtypes = [P, P, I64, I64, P, P]
+        getattr(lib, f"hpcs_partition_radix_{t}").argtypes = [P, P, I64, I64, P, I64]
+        getattr(lib, f"hpcs_select_radix_{t}").argtypes = [P, P, I64, I64, I64, P]
     lib.hpcs_histogram_byte_components_dev.argtypes = [P, I32, P, I64, P, P]
     lib.hpcs_shard_partition_dev.argtypes = [P, I32, P, P, I64, I64, P, P, I32, P, P, P, P]
     for t in COUNT_NP_OF:
@@ -334,6 +336,21 @@ class Context:
         t = dtype_name(a.dtype)
         check(getattr(self.lib, f"hpcs_select_topk_{t}")(self.handle, _ptr(a), a.size, k))
         return a
+
+    def partition_radix(self, a: np.ndarray, start: int, length: int, ks) -> np.ndarray:
+        """PartitionRadix over a[start, start + length) by the absolute indices ks, in place."""
+        t = dtype_name(a.dtype)
+        kk = np.ascontiguousarray(np.atleast_1d(np.asarray(ks, dtype=np.int64)))
+        check(getattr(self.lib, f"hpcs_partition_radix_{t}")(self.handle, _ptr(a), start, length,
+                                                               kk.ctypes.data if kk.size else None, kk.size))
+        return a
+
+    def select_radix(self, a: np.ndarray, start: int, length: int, k: int):
+        """SelectRadix(Par): the k-th smallest key of a[start, start + length) (k absolute), left at a[k]."""
+        t = dtype_name(a.dtype)
+        out = np.zeros(1, dtype=a.dtype)
+        check(getattr(self.lib, f"hpcs_select_radix_{t}")(self.handle, _ptr(a), start, length, k, _ptr(out)))
+        return out[0]
 
     def topk_largest(self, a: np.ndarray, k: int) -> np.ndarray:
         """The k largest keys of a, ascending."""

@@ -295,6 +295,36 @@ int hpcs_topk_largest_u64_dev(hpcs_ctx* ctx, const uint64_t* in, int64_t n, int6
 int hpcs_topk_largest_i64_dev(hpcs_ctx* ctx, const int64_t* in, int64_t n, int64_t k, int64_t* out, void* stream);
 int hpcs_topk_largest_f64_dev(hpcs_ctx* ctx, const double* in, int64_t n, int64_t k, double* out, void* stream);
 
+/* ---- radix partition and selection by index --------------------------------------------
+ * Algorithm.PartitionRadix(this uint[] a, int start, int length, int k, int threshold)
+ * PartitionRadix.cs:135-147, (a, k) :155-164, and the k[] forms (a, start, length, int[] k)
+ * :173-190, (a, int[] k) :198-210 (the ulong versions share them): in place, afterwards every
+ * a[k_i] holds the key the sorted subarray a[start, start + length) has at index k_i, and the
+ * keys between two consecutive indices (or an index and an end of the subarray) lie between
+ * their keys, as C++'s nth_element does.  k indexes the whole array; the indices may come in any
+ * order and repeat.  The threshold of the reference's base case is a CPU tuning knob with no
+ * meaning here.  The order of keys inside each part is unspecified (the reference's is not
+ * stable either).  start < 0, length <= 0, nk < 0 or an index outside the subarray ->
+ * HPCS_ERR_RANGE; nk == 0 does nothing.  Up to 4 distinct indices are placed by radix selects
+ * and three-way partitions; more sort the subarray. */
+int hpcs_partition_radix_u32(hpcs_ctx* ctx, uint32_t* a, int64_t start, int64_t length, const int64_t* k, int64_t nk);
+int hpcs_partition_radix_i32(hpcs_ctx* ctx, int32_t* a, int64_t start, int64_t length, const int64_t* k, int64_t nk);
+int hpcs_partition_radix_f32(hpcs_ctx* ctx, float* a, int64_t start, int64_t length, const int64_t* k, int64_t nk);
+int hpcs_partition_radix_u64(hpcs_ctx* ctx, uint64_t* a, int64_t start, int64_t length, const int64_t* k, int64_t nk);
+int hpcs_partition_radix_i64(hpcs_ctx* ctx, int64_t* a, int64_t start, int64_t length, const int64_t* k, int64_t nk);
+int hpcs_partition_radix_f64(hpcs_ctx* ctx, double* a, int64_t start, int64_t length, const int64_t* k, int64_t nk);
+/* ParallelAlgorithm.SelectRadixPar(this uint[] a, int start, int length, int k, int
+ * parallelThreshold) SelectionRadixParallel.cs:254-266 and (a, k) :271-283, and the serial
+ * Algorithm.SelectRadix(this uint[], start, length, k) SelectionRadix.cs:236-250: *out = the
+ * k-th smallest key of a[start, start + length) (k absolute), which is also left at a[k]; the
+ * subarray is partitioned around it as by hpcs_partition_radix_<t> with one index. */
+int hpcs_select_radix_u32(hpcs_ctx* ctx, uint32_t* a, int64_t start, int64_t length, int64_t k, uint32_t* out);
+int hpcs_select_radix_i32(hpcs_ctx* ctx, int32_t* a, int64_t start, int64_t length, int64_t k, int32_t* out);
+int hpcs_select_radix_f32(hpcs_ctx* ctx, float* a, int64_t start, int64_t length, int64_t k, float* out);
+int hpcs_select_radix_u64(hpcs_ctx* ctx, uint64_t* a, int64_t start, int64_t length, int64_t k, uint64_t* out);
+int hpcs_select_radix_i64(hpcs_ctx* ctx, int64_t* a, int64_t start, int64_t length, int64_t k, int64_t* out);
+int hpcs_select_radix_f64(hpcs_ctx* ctx, double* a, int64_t start, int64_t length, int64_t k, double* out);
+
 /* ---- serving: continuous batching of sort and top-k requests ---------------------------
  * No reference counterpart (HPCsharp is a synchronous library).  Requests of any size and
  * dtype are submitted at any time from any thread; a scheduler thread admits each one as

@@ -67,6 +67,12 @@ struct Fn<uint32_t> {
   static int hist(hpcs_ctx* c, const uint32_t* a, int64_t l, int64_t r, uint32_t* o) {
     return hpcs_histogram_byte_components_u32(c, a, l, r, o);
   }
+  static int partition(hpcs_ctx* c, uint32_t* a, int64_t start, int64_t length, const int64_t* k, int64_t nk) {
+    return hpcs_partition_radix_u32(c, a, start, length, k, nk);
+  }
+  static int select(hpcs_ctx* c, uint32_t* a, int64_t start, int64_t length, int64_t k, uint32_t* out) {
+    return hpcs_select_radix_u32(c, a, start, length, k, out);
+  }
 };
 template <>
 struct Fn<int32_t> {
@@ -74,6 +80,12 @@ struct Fn<int32_t> {
   static int pairs(hpcs_ctx* c, int32_t* k, uint32_t* v, int64_t n) { return hpcs_sort_pairs_i32(c, k, v, n); }
   static int hist(hpcs_ctx* c, const int32_t* a, int64_t l, int64_t r, uint32_t* o) {
     return hpcs_histogram_byte_components_i32(c, a, l, r, o);
+  }
+  static int partition(hpcs_ctx* c, int32_t* a, int64_t start, int64_t length, const int64_t* k, int64_t nk) {
+    return hpcs_partition_radix_i32(c, a, start, length, k, nk);
+  }
+  static int select(hpcs_ctx* c, int32_t* a, int64_t start, int64_t length, int64_t k, int32_t* out) {
+    return hpcs_select_radix_i32(c, a, start, length, k, out);
   }
 };
 template <>
@@ -83,6 +95,12 @@ struct Fn<float> {
   static int hist(hpcs_ctx* c, const float* a, int64_t l, int64_t r, uint32_t* o) {
     return hpcs_histogram_byte_components_f32(c, a, l, r, o);
   }
+  static int partition(hpcs_ctx* c, float* a, int64_t start, int64_t length, const int64_t* k, int64_t nk) {
+    return hpcs_partition_radix_f32(c, a, start, length, k, nk);
+  }
+  static int select(hpcs_ctx* c, float* a, int64_t start, int64_t length, int64_t k, float* out) {
+    return hpcs_select_radix_f32(c, a, start, length, k, out);
+  }
 };
 template <>
 struct Fn<uint64_t> {
@@ -90,6 +108,12 @@ struct Fn<uint64_t> {
   static int pairs(hpcs_ctx* c, uint64_t* k, uint32_t* v, int64_t n) { return hpcs_sort_pairs_u64(c, k, v, n); }
   static int hist(hpcs_ctx* c, const uint64_t* a, int64_t l, int64_t r, uint32_t* o) {
     return hpcs_histogram_byte_components_u64(c, a, l, r, o);
+  }
+  static int partition(hpcs_ctx* c, uint64_t* a, int64_t start, int64_t length, const int64_t* k, int64_t nk) {
+    return hpcs_partition_radix_u64(c, a, start, length, k, nk);
+  }
+  static int select(hpcs_ctx* c, uint64_t* a, int64_t start, int64_t length, int64_t k, uint64_t* out) {
+    return hpcs_select_radix_u64(c, a, start, length, k, out);
   }
 };
 template <>
@@ -99,6 +123,12 @@ struct Fn<int64_t> {
   static int hist(hpcs_ctx* c, const int64_t* a, int64_t l, int64_t r, uint32_t* o) {
     return hpcs_histogram_byte_components_i64(c, a, l, r, o);
   }
+  static int partition(hpcs_ctx* c, int64_t* a, int64_t start, int64_t length, const int64_t* k, int64_t nk) {
+    return hpcs_partition_radix_i64(c, a, start, length, k, nk);
+  }
+  static int select(hpcs_ctx* c, int64_t* a, int64_t start, int64_t length, int64_t k, int64_t* out) {
+    return hpcs_select_radix_i64(c, a, start, length, k, out);
+  }
 };
 template <>
 struct Fn<double> {
@@ -106,6 +136,12 @@ struct Fn<double> {
   static int pairs(hpcs_ctx* c, double* k, uint32_t* v, int64_t n) { return hpcs_sort_pairs_f64(c, k, v, n); }
   static int hist(hpcs_ctx* c, const double* a, int64_t l, int64_t r, uint32_t* o) {
     return hpcs_histogram_byte_components_f64(c, a, l, r, o);
+  }
+  static int partition(hpcs_ctx* c, double* a, int64_t start, int64_t length, const int64_t* k, int64_t nk) {
+    return hpcs_partition_radix_f64(c, a, start, length, k, nk);
+  }
+  static int select(hpcs_ctx* c, double* a, int64_t start, int64_t length, int64_t k, double* out) {
+    return hpcs_select_radix_f64(c, a, start, length, k, out);
   }
 };
 template <class T>
@@ -153,9 +189,59 @@ struct ParallelAlgorithm {
     for (size_t d = 0; d < sizeof(T); d++) out[d].assign(flat.begin() + d * 256, flat.begin() + (d + 1) * 256);
     return out;
   }
+  // SelectRadixPar(this uint[], int start, int length, int k, int parallelThreshold)
+  // SelectionRadixParallel.cs:254 and (a, k) :271: the k-th smallest of the (sub)array, k
+  // absolute, also left at a[k].  The threshold is a CPU task size with no meaning on the GPU.
+  template <class T>
+  static T SelectRadixPar(std::vector<T>& a, int64_t start, int64_t length, int64_t k,
+                          int parallelThreshold = 64 * 1024) {
+    (void)parallelThreshold;
+    if (start < 0 || length <= 0 || start + length > int64_t(a.size()))
+      throw ArgumentOutOfRangeException("array length or length is invalid");
+    T out{};
+    detail::Context& c = detail::context();
+    std::lock_guard<std::mutex> lock(c.mu);
+    detail::check(detail::Fn<T>::select(c.get(), a.data(), start, length, k, &out));
+    return out;
+  }
+  template <class T>
+  static T SelectRadixPar(std::vector<T>& a, int64_t k, int parallelThreshold = 64 * 1024) {
+    return SelectRadixPar(a, 0, int64_t(a.size()), k, parallelThreshold);
+  }
 };
 
 struct Algorithm {
+  // PartitionRadix(this uint[], int start, int length, int[] k, int threshold) PartitionRadix.cs:
+  // 135-210 (and the one-k and whole-array forms): nth_element by every k (absolute indices).
+  template <class T>
+  static void PartitionRadix(std::vector<T>& a, int64_t start, int64_t length, const std::vector<int64_t>& k,
+                             int threshold = 1024) {
+    (void)threshold;
+    if (start < 0 || length <= 0 || start + length > int64_t(a.size()))
+      throw ArgumentOutOfRangeException("array length or length is invalid");
+    if (k.size() > a.size()) throw ArgumentOutOfRangeException("k array length cannot be greater than the array length");
+    if (k.empty()) return;
+    detail::Context& c = detail::context();
+    std::lock_guard<std::mutex> lock(c.mu);
+    detail::check(detail::Fn<T>::partition(c.get(), a.data(), start, length, k.data(), int64_t(k.size())));
+  }
+  template <class T>
+  static void PartitionRadix(std::vector<T>& a, int64_t k, int threshold = 1024) {
+    PartitionRadix(a, 0, int64_t(a.size()), std::vector<int64_t>{k}, threshold);
+  }
+  template <class T>
+  static void PartitionRadix(std::vector<T>& a, const std::vector<int64_t>& k, int threshold = 1024) {
+    PartitionRadix(a, 0, int64_t(a.size()), k, threshold);
+  }
+  // SelectRadix(this uint[], int start, int length, int k) SelectionRadix.cs:236 and (a, k) :253
+  template <class T>
+  static T SelectRadix(std::vector<T>& a, int64_t start, int64_t length, int64_t k) {
+    return ParallelAlgorithm::SelectRadixPar(a, start, length, k);
+  }
+  template <class T>
+  static T SelectRadix(std::vector<T>& a, int64_t k) {
+    return ParallelAlgorithm::SelectRadixPar(a, 0, int64_t(a.size()), k);
+  }
   // SortRadixLsd(this T[]) RadixSortLsd.cs:255, :352, :437, :527 (in place)
   template <class T>
   static void SortRadixLsd(std::vector<T>& inOutArray) {

@@ -62,6 +62,8 @@ def lib():
         L.orc_sort_radix_par_ws_k32.argtypes = [P, P, I64, I, I]
         L.orc_sort_radix_par_ws_k64.argtypes = [P, P, I64, I, I]
         L.orc_gen_u32_uniform.argtypes = [P, I64, C.c_uint64, I]
+        for w in ("k32", "k64"):
+            getattr(L, f"orc_partition_radix_{w}").argtypes = [P, I64, I64, P, I64, I, I64]
         _lib = L
     return _lib
 
@@ -166,6 +168,15 @@ def histogram_byte_components(a: np.ndarray, l: int, r: int, parallel: bool = Fa
 def select_topk(a: np.ndarray, k: int) -> int:
     """SelectTopK(a, k) restatement (SelectionTopKRadix.cs:96-171), in place."""
     return getattr(lib(), f"orc_select_topk_{_w(a)}")(a.ctypes.data, a.size, k, KIND[_name(a)])
+
+
+def partition_radix(a: np.ndarray, start: int, length: int, ks, threshold: int = 1024) -> np.ndarray:
+    """PartitionRadix(a, start, length, k or k[], threshold) restatement (PartitionRadix.cs:15-210),
+    in place; ks are absolute indices in ascending order."""
+    kk = np.ascontiguousarray(np.atleast_1d(np.asarray(ks, dtype=np.int64)))
+    getattr(lib(), f"orc_partition_radix_{_w(a)}")(a.ctypes.data, start, length, kk.ctypes.data, kk.size,
+                                                   KIND[_name(a)], threshold)
+    return a
 
 
 def stable_sort_transformed(a: np.ndarray) -> np.ndarray:

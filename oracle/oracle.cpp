@@ -452,6 +452,65 @@ int select_topk(T* a, int64_t n, int64_t k, int kind) {
   return rc;
 }
 
+// ---------------------------------------------------------------------------------
+// PartitionRadix(this uint[] a, int start, int length, int k / int[] k, int threshold = 1024)
+// PartitionRadix.cs:135-210 with PartitionRadixMsdUIntInner (:15-63, the ulong twin :64-113).
+// In place, MSD by 8-bit digits from the top: histogram of the current digit over
+// [start, start + length) (HistogramOneByteComponent), bin starts, then the cycle-leader swap
+// loop that moves every element into its bin (:32-41), then recursion into the bins that hold
+// one of the k indices (:47-61).  A range shorter than `threshold` is sorted by the base case
+// (Array.Sort, restated as std::sort on the order-transformed key).  Observable contract (what
+// parity compares; the order inside each part is not): a[k_i] is the element the sorted
+// subarray has at k_i, and every element between two consecutive k's (or a k and an end of the
+// subarray) lies between their values.  k indexes the whole array; the k's ascend.
+// ---------------------------------------------------------------------------------
+template <class U>
+void partition_radix_inner(U* a, int64_t start, int64_t length, int shift, const int64_t* k, int64_t kstart,
+                           int64_t klength, int64_t threshold) {
+  if (length < threshold) {
+    std::sort(a + start, a + start + length);
+    return;
+  }
+  const int64_t last = start + length - 1;
+  int64_t count[256] = {0};
+  for (int64_t i = start; i <= last; i++) count[(a[i] >> shift) & 0xFF]++;
+  int64_t sob[257], eob[256];
+  sob[0] = eob[0] = start;
+  sob[256] = -1;  // sentinel (:28)
+  for (int b = 1; b < 256; b++) sob[b] = eob[b] = sob[b - 1] + count[b - 1];
+  int next_bin = 1;
+  for (int64_t cur = start; cur <= last;) {
+    U e = a[cur];
+    unsigned d;
+    while (eob[d = unsigned((e >> shift) & 0xFF)] != cur) std::swap(e, a[eob[d]++]);
+    a[cur] = e;
+    eob[d]++;
+    while (next_bin < 256 && eob[next_bin - 1] == sob[next_bin]) next_bin++;
+    cur = eob[next_bin - 1];
+  }
+  if (shift > 0) {
+    const int nshift = shift >= 8 ? shift - 8 : 0;
+    for (int b = 0, ki = int(kstart); b < 256 && ki < kstart + klength; b++) {
+      if (sob[b] <= eob[b] && k[ki] >= sob[b] && k[ki] < eob[b]) {
+        const int64_t ks = ki++;
+        int64_t kl = 1;
+        for (; ki < kstart + klength; ki++) {
+          if (k[ki] >= sob[b] && k[ki] < eob[b]) kl++;
+          else break;
+        }
+        partition_radix_inner<U>(a, sob[b], eob[b] - sob[b], nshift, k, ks, kl, threshold);
+      }
+    }
+  }
+}
+
+template <class U>
+void partition_radix(U* a, int64_t start, int64_t length, const int64_t* k, int64_t nk, int kind, int64_t threshold) {
+  for (int64_t i = start; i < start + length; i++) a[i] = order_bits<U>(a[i], kind);
+  if (nk > 0) partition_radix_inner<U>(a, start, length, int(sizeof(U) * 8 - 8), k, 0, nk, threshold);
+  for (int64_t i = start; i < start + length; i++) a[i] = order_bits_inverse<U>(a[i], kind);
+}
+
 // std::sort stand-in for Array.Sort (introsort) on integer keys, and std::stable_sort on the
 // transformed key for the cross-checks.
 template <class U>
@@ -581,6 +640,16 @@ int orc_select_topk_k32(uint32_t* a, int64_t n, int64_t k, int kind) {
 }
 int orc_select_topk_k64(uint64_t* a, int64_t n, int64_t k, int kind) {
   return select_topk<uint64_t, uint64_t>(a, n, k, kind);
+}
+
+// PartitionRadix over [start, start + length) by the ascending indices k[0..nk) (absolute).
+void orc_partition_radix_k32(uint32_t* a, int64_t start, int64_t length, const int64_t* k, int64_t nk, int kind,
+                             int64_t threshold) {
+  partition_radix<uint32_t>(a, start, length, k, nk, kind, threshold);
+}
+void orc_partition_radix_k64(uint64_t* a, int64_t start, int64_t length, const int64_t* k, int64_t nk, int kind,
+                             int64_t threshold) {
+  partition_radix<uint64_t>(a, start, length, k, nk, kind, threshold);
 }
 
 // Cross-check helpers.

@@ -103,6 +103,24 @@ int main() {
   }
   CHECK(threw);
 
+  // PartitionRadix / SelectRadixPar: nth_element by each index, checked against std::sort
+  {
+    std::vector<uint32_t> p(500009);
+    for (auto& x : p) x = uint32_t(rng()) & 0xFFFFu;  // many equal keys
+    std::vector<uint32_t> sorted = p;
+    std::sort(sorted.begin(), sorted.end());
+    std::vector<int64_t> ks = {7, 250000, 499999};
+    std::vector<uint32_t> q = p;
+    Algorithm::PartitionRadix(q, ks);
+    for (int64_t k : ks) CHECK(q[k] == sorted[k]);
+    for (int64_t i = 0; i < 7; i++) CHECK(q[i] <= q[7]);
+    for (int64_t i = 8; i < 250000; i++) CHECK(q[i] >= q[7] && q[i] <= q[250000]);
+    std::vector<uint32_t> r = p;
+    CHECK(ParallelAlgorithm::SelectRadixPar(r, 123456) == sorted[123456]);
+    CHECK(r[123456] == sorted[123456]);
+    CHECK(Algorithm::SelectRadix(p, 0) == sorted[0]);
+  }
+
   std::printf(failures ? "mirror_test: %d failures\n" : "mirror_test: ok\n", failures);
   return failures ? 1 : 0;
 }
