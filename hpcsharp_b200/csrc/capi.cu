@@ -14,6 +14,7 @@
 #include "segmented_host.cuh"
 #include "topk_host.cuh"
 #include "shard.cuh"
+#include "host_copy.cuh"
 
 namespace hpcs {
 
@@ -172,10 +173,9 @@ int sort_host(hpcs_ctx* ctx, T* keys, int64_t n) {
   if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
   if ((rc = ensure(ctx, ctx->keys_a, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
   U* d = static_cast<U*>(ctx->keys_a.ptr);
-  HPCS_CUDA(cudaMemcpyAsync(d, keys, size_t(n) * sizeof(U), cudaMemcpyHostToDevice, s));
+  if ((rc = copy_to_device(ctx, d, keys, size_t(n) * sizeof(U), s)) != HPCS_OK) return rc;
   if ((rc = enqueue_sort<U, KIND, NoValue>(ctx, d, nullptr, n, s)) != HPCS_OK) return rc;
-  HPCS_CUDA(cudaMemcpyAsync(keys, d, size_t(n) * sizeof(U), cudaMemcpyDeviceToHost, s));
-  HPCS_CUDA(cudaStreamSynchronize(s));
+  if ((rc = copy_to_host(ctx, keys, d, size_t(n) * sizeof(U), s)) != HPCS_OK) return rc;
   return check_device_errors(ctx);
 }
 
@@ -240,10 +240,9 @@ int count_sort_host(hpcs_ctx* ctx, T* keys, int64_t n, uint32_t flip) {
   if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
   if ((rc = ensure(ctx, ctx->keys_a, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
   U* d = static_cast<U*>(ctx->keys_a.ptr);
-  HPCS_CUDA(cudaMemcpyAsync(d, keys, size_t(n) * sizeof(U), cudaMemcpyHostToDevice, s));
+  if ((rc = copy_to_device(ctx, d, keys, size_t(n) * sizeof(U), s)) != HPCS_OK) return rc;
   if ((rc = enqueue_count_sort<U>(ctx, d, n, flip, s)) != HPCS_OK) return rc;
-  HPCS_CUDA(cudaMemcpyAsync(keys, d, size_t(n) * sizeof(U), cudaMemcpyDeviceToHost, s));
-  HPCS_CUDA(cudaStreamSynchronize(s));
+  if ((rc = copy_to_host(ctx, keys, d, size_t(n) * sizeof(U), s)) != HPCS_OK) return rc;
   return check_device_errors(ctx);
 }
 
@@ -270,12 +269,11 @@ int pairs_host(hpcs_ctx* ctx, T* keys, uint32_t* items, int64_t n) {
   if ((rc = ensure(ctx, ctx->vals_a, size_t(n) * 4)) != HPCS_OK) return rc;
   U* dk = static_cast<U*>(ctx->keys_a.ptr);
   uint32_t* dv = static_cast<uint32_t*>(ctx->vals_a.ptr);
-  HPCS_CUDA(cudaMemcpyAsync(dk, keys, size_t(n) * sizeof(U), cudaMemcpyHostToDevice, s));
-  HPCS_CUDA(cudaMemcpyAsync(dv, items, size_t(n) * 4, cudaMemcpyHostToDevice, s));
+  if ((rc = copy_to_device(ctx, dk, keys, size_t(n) * sizeof(U), s)) != HPCS_OK) return rc;
+  if ((rc = copy_to_device(ctx, dv, items, size_t(n) * 4, s)) != HPCS_OK) return rc;
   if ((rc = enqueue_sort<U, KIND, uint32_t>(ctx, dk, dv, n, s)) != HPCS_OK) return rc;
-  HPCS_CUDA(cudaMemcpyAsync(keys, dk, size_t(n) * sizeof(U), cudaMemcpyDeviceToHost, s));
-  HPCS_CUDA(cudaMemcpyAsync(items, dv, size_t(n) * 4, cudaMemcpyDeviceToHost, s));
-  HPCS_CUDA(cudaStreamSynchronize(s));
+  if ((rc = copy_to_host(ctx, keys, dk, size_t(n) * sizeof(U), s)) != HPCS_OK) return rc;
+  if ((rc = copy_to_host(ctx, items, dv, size_t(n) * 4, s)) != HPCS_OK) return rc;
   return check_device_errors(ctx);
 }
 
@@ -330,7 +328,7 @@ int histogram_host(hpcs_ctx* ctx, const T* a, int64_t l, int64_t r, uint32_t* co
   if ((rc = ensure(ctx, ctx->counts, size_t(MAX_PASSES) * RADIX * 4)) != HPCS_OK) return rc;
   U* d = static_cast<U*>(ctx->keys_a.ptr);
   uint32_t* dc = static_cast<uint32_t*>(ctx->counts.ptr);
-  HPCS_CUDA(cudaMemcpyAsync(d, a + l, size_t(n) * sizeof(U), cudaMemcpyHostToDevice, s));
+  if ((rc = copy_to_device(ctx, d, a + l, size_t(n) * sizeof(U), s)) != HPCS_OK) return rc;
   if ((rc = enqueue_histogram<U, KIND>(ctx, d, n, dc, s)) != HPCS_OK) return rc;
   HPCS_CUDA(cudaMemcpyAsync(counts, dc, size_t(P) * RADIX * 4, cudaMemcpyDeviceToHost, s));
   HPCS_CUDA(cudaStreamSynchronize(s));
@@ -359,12 +357,11 @@ int select_topk_host(hpcs_ctx* ctx, T* a, int64_t n, int64_t k) {
   if ((rc = ensure(ctx, ctx->keys_b, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
   U* d = static_cast<U*>(ctx->keys_a.ptr);
   U* o = static_cast<U*>(ctx->keys_b.ptr);
-  HPCS_CUDA(cudaMemcpyAsync(d, a, size_t(n) * sizeof(U), cudaMemcpyHostToDevice, s));
+  if ((rc = copy_to_device(ctx, d, a, size_t(n) * sizeof(U), s)) != HPCS_OK) return rc;
   SelectState* st = nullptr;
   if ((rc = enqueue_select<U, KIND>(ctx, d, n, k, s, &st)) != HPCS_OK) return rc;
   if ((rc = enqueue_partition<U, KIND>(ctx, d, n, st, o, s)) != HPCS_OK) return rc;
-  HPCS_CUDA(cudaMemcpyAsync(a, o, size_t(n) * sizeof(U), cudaMemcpyDeviceToHost, s));
-  HPCS_CUDA(cudaStreamSynchronize(s));
+  if ((rc = copy_to_host(ctx, a, o, size_t(n) * sizeof(U), s)) != HPCS_OK) return rc;
   return check_device_errors(ctx);
 }
 
@@ -446,10 +443,9 @@ int partition_radix_host(hpcs_ctx* ctx, T* a, int64_t start, int64_t length, con
   if ((rc = ensure(ctx, ctx->vals_a, size_t(length) * sizeof(U))) != HPCS_OK) return rc;
   U* d = static_cast<U*>(ctx->keys_a.ptr);
   U* o = static_cast<U*>(ctx->vals_a.ptr);
-  HPCS_CUDA(cudaMemcpyAsync(d, a + start, size_t(length) * sizeof(U), cudaMemcpyHostToDevice, s));
+  if ((rc = copy_to_device(ctx, d, a + start, size_t(length) * sizeof(U), s)) != HPCS_OK) return rc;
   if ((rc = enqueue_partition_ranks<U, KIND>(ctx, d, o, length, r, s)) != HPCS_OK) return rc;
-  HPCS_CUDA(cudaMemcpyAsync(a + start, d, size_t(length) * sizeof(U), cudaMemcpyDeviceToHost, s));
-  HPCS_CUDA(cudaStreamSynchronize(s));
+  if ((rc = copy_to_host(ctx, a + start, d, size_t(length) * sizeof(U), s)) != HPCS_OK) return rc;
   return check_device_errors(ctx);
 }
 
@@ -493,7 +489,7 @@ int topk_largest_host(hpcs_ctx* ctx, const T* in, int64_t n, int64_t k, T* out) 
   if ((rc = ensure(ctx, ctx->vals_a, size_t(k) * sizeof(U))) != HPCS_OK) return rc;
   U* d = static_cast<U*>(ctx->keys_a.ptr);
   U* o = static_cast<U*>(ctx->vals_a.ptr);
-  HPCS_CUDA(cudaMemcpyAsync(d, in, size_t(n) * sizeof(U), cudaMemcpyHostToDevice, s));
+  if ((rc = copy_to_device(ctx, d, in, size_t(n) * sizeof(U), s)) != HPCS_OK) return rc;
   if ((rc = topk_largest_enqueue<T, U, KIND>(ctx, d, n, k, o, s)) != HPCS_OK) return rc;
   HPCS_CUDA(cudaMemcpyAsync(out, o, size_t(k) * sizeof(U), cudaMemcpyDeviceToHost, s));
   HPCS_CUDA(cudaStreamSynchronize(s));
@@ -593,6 +589,7 @@ void hpcs_config_default(hpcs_config* cfg) {
   cfg->spin_limit_ns = 2000000000LL;
   cfg->poison_tile = -1;
   cfg->rank_mode = 0;
+  cfg->staged_host_copies = 1;
 }
 
 int hpcs_abi_version(void) { return HPCS_ABI_VERSION; }
@@ -686,6 +683,7 @@ int hpcs_ctx_destroy(hpcs_ctx* ctx) {
     if (ctx->seg_join[b]) cudaEventDestroy(ctx->seg_join[b]);
   }
   if (ctx->seg_fork) cudaEventDestroy(ctx->seg_fork);
+  delete ctx->stager;
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return HPCS_OK;

@@ -36,6 +36,10 @@ struct DevBuf {
 
 }  // namespace hpcs
 
+namespace hpcs {
+struct HostStager;
+}
+
 struct hpcs_ctx {
   int device = 0;
   int sms = 0;
@@ -61,6 +65,8 @@ struct hpcs_ctx {
   hpcs::DevBuf keys_a, keys_b, vals_a, vals_b, status0, status1, plan, counts, err_accum;
   hpcs::DevBuf status2;  // second look-back buffer when the device chooses the scheme
   hpcs::DevBuf aux0, aux1, aux2;
+  // pinned ring and copy threads for host arrays in pageable memory (host_copy.cuh)
+  hpcs::HostStager* stager = nullptr;
   // batched segmented sort: variant per (key width, length class), and the helper streams
   // and events that run the launches of different variants concurrently
   hpcs_seg_tuning seg_tuning{};

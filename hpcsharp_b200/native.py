@@ -74,7 +74,8 @@ class HpcsConfig(C.Structure):
         ("spin_limit_ns", C.c_int64),
         ("poison_tile", C.c_int32),
         ("pass_scheme", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("staged_host_copies", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -251,9 +252,10 @@ class Context:
 
     def __init__(self, device: int = 0, *, pool_bytes: int = 0, skip_trivial_passes: bool = True,
                  spin_limit_ns: int = 2_000_000_000, poison_tile: int = -1, rank_mode: int = 0,
-                 pass_scheme: str = "auto"):
+                 pass_scheme: str = "auto", staged_host_copies: bool = True):
         self.lib = load()
         cfg = default_config()
+        cfg.staged_host_copies = 1 if staged_host_copies else 0
         cfg.pool_bytes = pool_bytes
         cfg.skip_trivial_passes = 1 if skip_trivial_passes else 0
         cfg.spin_limit_ns = spin_limit_ns

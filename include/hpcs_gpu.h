@@ -83,7 +83,11 @@ typedef struct hpcs_config {
                                   type and n; HPCS_PASSES_LOOKBACK (1): single-pass decoupled
                                   look-back; HPCS_PASSES_CHUNKED (2): per-range counts from
                                   the previous pass, no inter-CTA waiting */
-  int32_t reserved[6];
+  int32_t staged_host_copies;  /* host-array calls on pageable memory (default 1): copy through
+                                  the context's pinned buffers in chunks, several host threads
+                                  copying while the DMA engine moves earlier chunks; 0: one
+                                  cudaMemcpyAsync per array (the driver stages it) */
+  int32_t reserved[5];
 } hpcs_config;
 
 /* ---- context ---------------------------------------------------------------------- */
