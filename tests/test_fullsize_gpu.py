@@ -124,3 +124,31 @@ def test_sort_beyond_2_to_30_keys(ctx):
     assert bool((idx[1:][same] > idx[:-1][same]).all())
     del keys, orig, items, idx, same
     torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("dt,n,gen", PAIRS, ids=["u64_zipf_200M_pairs", "f64_normal_100M_pairs"])
+def test_pairs_at_scale_both_rank_modes(ctx, dt, n, gen):
+    """The shipping context ranks with ordered shared atomics when its probe passed; the
+    peer-mask mode is fully defined by PTX.  Both must give the identical keys and stable
+    permutation on the full-size pairs configurations (heavy duplicates: many same-address
+    atomics per warp instruction)."""
+    import torch
+
+    peer = native.Context(0, rank_mode=1)
+    try:
+        a = gen(n)
+        out = {}
+        for name, c in (("ctx", ctx), ("peer", peer)):
+            keys = to_dev(a)
+            items = torch.arange(n, dtype=torch.int32, device="cuda")
+            c.sort_pairs_dev(keys, items, dtype=dt, stream=native.torch_stream())
+            torch.cuda.synchronize()
+            c.synchronize()
+            out[name] = (keys, items)
+        assert peer.rank_mode == 1
+        assert torch.equal(out["ctx"][0], out["peer"][0])
+        assert torch.equal(out["ctx"][1], out["peer"][1])
+        del out
+        torch.cuda.empty_cache()
+    finally:
+        peer.close()

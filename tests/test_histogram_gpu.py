@@ -120,9 +120,12 @@ def test_histogram_device_parity(ctx, orc, dt, offset):
 def test_histogram_device_empty_zeroes_counts(ctx):
     import torch
 
-    t = torch.empty(0, dtype=torch.int32, device="cuda")
+    lib = native.load()
+    keys = torch.zeros(16, dtype=torch.int32, device="cuda")  # a valid pointer, zero keys counted
     counts = torch.full((4 * 256,), 9, dtype=torch.int32, device="cuda")
-    ctx.histogram_dev(t, counts, dtype="u32", stream=native.torch_stream())
+    rc = lib.hpcs_histogram_byte_components_dev(ctx.handle, native.DTYPES["u32"], keys.data_ptr(), 0,
+                                                counts.data_ptr(), native.torch_stream())
+    assert rc == native.HPCS_OK
     torch.cuda.synchronize()
     ctx.synchronize()
     assert int(counts.abs().sum()) == 0
