@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--dtype", default="u32", choices=["u32", "i32", "f32", "u64", "i64", "f64"])
+    ap.add_argument("--scheme", default="auto", choices=["auto", "chunked", "lookback", "wide"],
+                    help="plain: the digit-pass scheme of the library (auto picks by key type and n)")
     ap.add_argument("--slots", type=int, default=4, help="distinct input copies cycled through")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps (capped at 20)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -287,7 +289,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     tview = {4: torch.int32, 8: torch.int64}[w]
     src = torch.from_numpy(host.view({4: np.int32, 8: np.int64}[w])).to(f"cuda:{dev}")
     slots = [src.clone() for _ in range(max(1, args.slots))]
-    ctx = native.Context(dev)
+    ctx = native.Context(dev, pass_scheme=args.scheme)
     s = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{dev}")
 
     def step(i):

@@ -141,6 +141,83 @@ int probe_rank_order(hpcs_ctx* ctx, int* ordered) {
   return HPCS_OK;
 }
 
+int check_device_errors(hpcs_ctx* ctx);
+
+// ---- probe of the shipping pass kernels ---------------------------------------------------
+// Keys whose digits (11-bit, so also every 8-bit digit) take few values, so many lanes of a warp
+// instruction share a counter: `values` = 20 keeps them below the grouped-ranking threshold, 3
+// sends the frequent values to the grouped ranking; items are the input positions.
+__global__ void probe_fill_kernel(uint32_t* keys, uint32_t* items, int64_t n, uint32_t values) {
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+    uint32_t x = uint32_t(i) * 0x9E3779B1u ^ 0x85EBCA6Bu;
+    x ^= x >> 15;
+    x *= 0x2C1B3C6Du;
+    x ^= x >> 12;
+    const uint32_t d0 = (x & 0xFFFFu) % values, d1 = (x >> 16) % values, d2 = (x * 0x27D4EB2Fu >> 8) % values;
+    keys[i] = d0 | (d1 << 11) | (d2 << 22);
+    if (items) items[i] = uint32_t(i);
+  }
+}
+
+// Counts positions where the keys descend or, with items, equal keys' items do not ascend.
+__global__ void probe_check_kernel(const uint32_t* keys, const uint32_t* items, int64_t n, uint32_t* bad) {
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  uint32_t v = 0;
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x + 1; i < n; i += stride) {
+    if (keys[i] < keys[i - 1]) v++;
+    else if (items && keys[i] == keys[i - 1] && items[i] <= items[i - 1]) v++;
+  }
+  if (v) atomicAdd(bad, v);
+}
+
+// Runs the shipping ordered-atomic pass kernels -- the wide passes and the chunked 8-bit passes,
+// keys only and with items -- on inputs with many equal digits per warp instruction and checks
+// the results for order and stability.  Any violation sends the context to the peer-mask
+// ranking, which is defined by PTX.  The same code generation and occupancy as a real sort: the
+// probe calls the sort's own enqueue functions.
+int probe_shipping_kernels(hpcs_ctx* ctx, int* ok) {
+  constexpr int64_t n = (int64_t(1) << 20) + 12345;
+  uint32_t *keys = nullptr, *items = nullptr, *bad = nullptr;
+  cudaError_t e = cudaMalloc(&keys, size_t(n) * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&items, size_t(n) * 4);
+  if (e == cudaSuccess) e = cudaMalloc(&bad, 4);
+  if (e == cudaSuccess) e = cudaMemset(bad, 0, 4);
+  int rc = e == cudaSuccess ? HPCS_OK : cuda_fail(e, "probe buffers");
+  const int saved_mode = ctx->rank_mode;
+  const int saved_scheme = ctx->cfg.pass_scheme;
+  ctx->rank_mode = RANK_ORDERED_ATOMIC;
+  cudaStream_t s = ctx->stream;
+  for (int scheme : {int(HPCS_PASSES_WIDE), int(HPCS_PASSES_CHUNKED)}) {
+    ctx->cfg.pass_scheme = scheme;
+    for (uint32_t values : {20u, 3u}) {
+      for (int with_items = 0; with_items < 2 && rc == HPCS_OK; with_items++) {
+        uint32_t* it = with_items ? items : nullptr;
+        probe_fill_kernel<<<ctx->sms * 4, 256, 0, s>>>(keys, it, n, values);
+        if ((e = cudaGetLastError()) != cudaSuccess) rc = cuda_fail(e, "probe fill");
+        if (rc == HPCS_OK)
+          rc = with_items ? enqueue_sort<uint32_t, KIND_UNSIGNED, uint32_t>(ctx, keys, items, n, s)
+                          : enqueue_sort<uint32_t, KIND_UNSIGNED, NoValue>(ctx, keys, nullptr, n, s);
+        if (rc == HPCS_OK) {
+          probe_check_kernel<<<ctx->sms * 4, 256, 0, s>>>(keys, it, n, bad);
+          if ((e = cudaGetLastError()) != cudaSuccess) rc = cuda_fail(e, "probe check");
+        }
+      }
+    }
+  }
+  ctx->rank_mode = saved_mode;
+  ctx->cfg.pass_scheme = saved_scheme;
+  uint32_t h = 1;
+  if (rc == HPCS_OK && (e = cudaStreamSynchronize(s)) != cudaSuccess) rc = cuda_fail(e, "probe");
+  if (rc == HPCS_OK && (e = cudaMemcpy(&h, bad, 4, cudaMemcpyDeviceToHost)) != cudaSuccess) rc = cuda_fail(e, "probe");
+  if (rc == HPCS_OK) rc = check_device_errors(ctx);
+  cudaFree(keys);
+  cudaFree(items);
+  cudaFree(bad);
+  *ok = rc == HPCS_OK && h == 0;
+  return rc;
+}
+
 // Reads and clears the accumulated device error bits (synchronous).
 int check_device_errors(hpcs_ctx* ctx) {
   uint32_t bits = 0;
@@ -655,7 +732,22 @@ int hpcs_ctx_create(int device, const hpcs_config* cfg, hpcs_ctx** out) {
       hpcs_ctx_destroy(ctx);
       return rc;
     }
-    if (ordered) ctx->rank_mode = RANK_ORDERED_ATOMIC;
+    if (ordered) {
+      // once per device and process, with the first context: the shipping kernels themselves
+      static std::mutex probe_mu;
+      static int shipping[64];  // 0 unknown, 1 passed, 2 failed
+      std::lock_guard<std::mutex> lock(probe_mu);
+      int& sp = shipping[device & 63];
+      if (sp == 0) {
+        int ok = 0;
+        if ((rc = probe_shipping_kernels(ctx, &ok)) != HPCS_OK) {
+          hpcs_ctx_destroy(ctx);
+          return rc;
+        }
+        sp = ok ? 1 : 2;
+      }
+      if (sp == 1) ctx->rank_mode = RANK_ORDERED_ATOMIC;
+    }
   }
   *out = ctx;
   return HPCS_OK;

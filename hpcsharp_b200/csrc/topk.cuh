@@ -37,8 +37,12 @@ struct SelectState {
   int64_t cand_count;  // candidates compacted after level 0
   unsigned long long gathered;  // keys > v written to the top-k output so far
   int64_t n_total;     // keys selected among
+  uint64_t threshold;  // top-k: ordered keys at or above it are the filter's candidates
+  int32_t mode;        // top-k: SEL_MODE_CAND (select among the candidates) or SEL_MODE_FULL
+  int32_t pad;
   uint32_t hist[256];
 };
+enum : int32_t { SEL_MODE_ANY = -1, SEL_MODE_FULL = 0, SEL_MODE_CAND = 1 };
 
 static __global__ void select_init_kernel(SelectState* st, int64_t rank, int64_t n) {
   const int tid = threadIdx.x;
@@ -51,6 +55,8 @@ static __global__ void select_init_kernel(SelectState* st, int64_t rank, int64_t
     st->eq = 0;
     st->cand_count = 0;
     st->gathered = 0;
+    st->threshold = 0;
+    st->mode = SEL_MODE_FULL;
   }
   if (tid < 256) st->hist[tid] = 0;
 }
@@ -111,10 +117,12 @@ struct WarpStage {
 // Histogram of the digit at `shift` over keys whose ordered bits match (prefix, mask).
 template <class U, int KIND>
 __global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) select_hist_kernel(const U* __restrict__ keys, const int64_t* n_ptr,
-                                                             int64_t n_fixed, SelectState* st, int shift) {
+                                                             int64_t n_fixed, SelectState* st, int shift,
+                                                             int only_mode = SEL_MODE_ANY) {
   using KO = KeyOrder<U, KIND>;
   constexpr int E = int(16 / sizeof(U));
   __shared__ uint32_t sh[256 * SEL_COPIES];
+  if (only_mode != SEL_MODE_ANY && st->mode != only_mode) return;  // the other top-k path ran
   const int tid = threadIdx.x, lane = tid & 31;
   for (int i = tid; i < 256 * SEL_COPIES; i += SEL_NT) sh[i] = 0;
   __syncthreads();
@@ -187,11 +195,13 @@ __global__ void __launch_bounds__(256) select_pick_kernel(SelectState* st, int s
 template <class U, int KIND>
 __global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) select_compact_kernel(const U* __restrict__ keys, int64_t n,
                                                                 U* __restrict__ cand, SelectState* st,
-                                                                U* __restrict__ out, int64_t k_out) {
+                                                                U* __restrict__ out, int64_t k_out,
+                                                                int only_mode = SEL_MODE_ANY) {
   using KO = KeyOrder<U, KIND>;
   constexpr int E = int(16 / sizeof(U));
   constexpr int CAP = 1024 / int(sizeof(U));  // 1 KiB per warp and buffer
   __shared__ U s_buf[2][SEL_NT / 32][CAP];
+  if (only_mode != SEL_MODE_ANY && st->mode != only_mode) return;  // the other top-k path ran
   const int warp = threadIdx.x >> 5;
   const U prefix = U(st->prefix), mask = U(st->mask);
   WarpStage<U, E, CAP> to_cand{s_buf[0][warp], 0u, cand, reinterpret_cast<unsigned long long*>(&st->cand_count),
@@ -210,6 +220,105 @@ __global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) select_compact_kernel
   });
   to_cand.flush();
   if (out) to_out.flush();
+}
+
+// ---- top-k with one read of the keys ---------------------------------------------------
+// A strided sample of the keys gives a threshold T that about m = TOPK_MARGIN(k) sampled keys
+// reach; one read of all keys then keeps the keys at or above T (the candidates).  When at
+// least k keys were kept, every one of the k largest is among them and the radix select runs
+// over the candidates only; otherwise (a sample far off, or tiny inputs) the select falls back
+// to the two reads of the full path.  The choice is made on the device (SelectState::mode):
+// the kernels of the path not taken return at their first instruction.
+constexpr int TOPK_SAMPLE = 8192;
+constexpr int TOPK_SAMPLE_NT = 1024;
+
+// One CTA: the ordered sample value of rank (S - m), S = TOPK_SAMPLE samples at stride n / S,
+// by an MSD radix select in shared memory.  Writes st->threshold (0 = keep every key).
+template <class U, int KIND>
+__global__ void __launch_bounds__(TOPK_SAMPLE_NT) topk_sample_kernel(const U* __restrict__ keys, int64_t n,
+                                                                     int64_t m, SelectState* st) {
+  using KO = KeyOrder<U, KIND>;
+  constexpr int BITS = int(sizeof(U) * 8);
+  constexpr int PER = TOPK_SAMPLE / TOPK_SAMPLE_NT;
+  __shared__ uint32_t hist[256];
+  __shared__ uint32_t s_bin, s_below;
+  const int tid = threadIdx.x;
+  if (n < int64_t(4) * TOPK_SAMPLE || m >= TOPK_SAMPLE) {  // too few keys to sample: keep them all
+    if (tid == 0) st->threshold = 0;
+    return;
+  }
+  const int64_t stride = n / TOPK_SAMPLE;
+  U o[PER];
+#pragma unroll
+  for (int q = 0; q < PER; q++) o[q] = KO::to_ordered(keys[int64_t(tid + q * TOPK_SAMPLE_NT) * stride]);
+  // rank (0-based, ascending) of the threshold among the samples
+  uint32_t rank = uint32_t(TOPK_SAMPLE - m);
+  U prefix = 0, mask = 0;
+  for (int shift = BITS - 8; shift >= 0; shift -= 8) {
+    if (tid < 256) hist[tid] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < PER; q++)
+      if ((o[q] & mask) == prefix) atomicAdd(&hist[uint32_t(o[q] >> shift) & 0xFFu], 1u);
+    __syncthreads();
+    if (tid == 0) {  // 256 bins: a serial scan is a few hundred cycles per level
+      uint32_t below = 0;
+      int bin = 255;
+      for (int b = 0; b < 256; b++) {
+        if (rank < below + hist[b]) {
+          bin = b;
+          break;
+        }
+        below += hist[b];
+      }
+      s_bin = uint32_t(bin);
+      s_below = below;
+    }
+    __syncthreads();
+    prefix |= U(s_bin) << shift;
+    mask |= U(0xFF) << shift;
+    rank -= s_below;
+    __syncthreads();
+  }
+  if (tid == 0) st->threshold = uint64_t(prefix);
+}
+
+// One read of the keys: the keys whose ordered value is at least the threshold go to `cand`.
+template <class U, int KIND>
+__global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) topk_filter_kernel(const U* __restrict__ keys, int64_t n,
+                                                             U* __restrict__ cand, SelectState* st) {
+  using KO = KeyOrder<U, KIND>;
+  constexpr int E = int(16 / sizeof(U));
+  constexpr int CAP = 1024 / int(sizeof(U));
+  __shared__ U s_buf[SEL_NT / 32][CAP];
+  const U t = U(st->threshold);
+  WarpStage<U, E, CAP> to_cand{s_buf[threadIdx.x >> 5], 0u, cand,
+                               reinterpret_cast<unsigned long long*>(&st->cand_count), INT64_MAX};
+  visit_keys<U, SEL_VPT>(keys, n, [&](const U* k, int nv) {
+    uint32_t take = 0u;
+#pragma unroll
+    for (int e = 0; e < E; e++)
+      if (e < nv && KO::to_ordered(k[e]) >= t) take |= 1u << e;
+    to_cand.add(k, take);
+  });
+  to_cand.flush();
+}
+
+// One thread: select among the candidates when there are at least k of them (rank cand - k),
+// else fall back to the full path over all n keys (rank n - k, the candidates rebuilt).
+static __global__ void topk_decide_kernel(SelectState* st, int64_t n, int64_t k) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int64_t c = st->cand_count;
+  if (c >= k) {
+    st->mode = SEL_MODE_CAND;
+    st->n_total = c;
+    st->rank = c - k;
+  } else {
+    st->mode = SEL_MODE_FULL;
+    st->n_total = n;
+    st->rank = n - k;
+    st->cand_count = 0;
+  }
 }
 
 // ---- stable three-way partition around the selected key -----------------------------

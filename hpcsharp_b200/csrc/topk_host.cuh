@@ -3,6 +3,8 @@
 // keys, aux1: SelectState, aux2: partition tile counts), which the serving runtime binds to
 // slices of its arena.
 #pragma once
+#include <cmath>
+
 #include "sort_host.cuh"
 #include "topk.cuh"
 
@@ -61,17 +63,40 @@ inline int enqueue_partition(hpcs_ctx* ctx, const U* d, int64_t n, SelectState* 
   return HPCS_OK;
 }
 
-// The k largest of in[0..n) into out[0..k), ascending (device pointers).
+// The k largest of in[0..n) into out[0..k), ascending (device pointers).  One read of the keys
+// in the common case: a sampled threshold, one filtering read, the radix select over the
+// candidates (topk.cuh); the two-read select over all keys when the candidates fall short.
 template <class T, class U, int KIND>
 inline int topk_largest_enqueue(hpcs_ctx* ctx, const U* d, int64_t n, int64_t k, U* out, cudaStream_t s) {
-  SelectState* st = nullptr;
+  constexpr int BITS = int(sizeof(U) * 8);
+  constexpr int LEVELS = BITS / 8;
   int rc;
-  if ((rc = enqueue_select<U, KIND>(ctx, d, n, n - k, s, &st, out)) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->aux1, sizeof(SelectState))) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->aux0, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
+  SelectState* st = static_cast<SelectState*>(ctx->aux1.ptr);
+  U* cand = static_cast<U*>(ctx->aux0.ptr);
+  const int grid = select_grid(ctx, n, int(sizeof(U)));
   {
-    // candidates: at most n of them, usually about n/256; the grid covers n
     KernelTimer kt(ctx, s, HPCS_K_TOPK);
-    const U* cand = static_cast<const U*>(ctx->aux0.ptr);
-    topk_gather_kernel<U, KIND><<<select_grid(ctx, n, int(sizeof(U))), SEL_NT, 0, s>>>(cand, k, st, out);
+    select_init_kernel<<<1, 256, 0, s>>>(st, n - k, n);
+    // sampled keys expected at or above the threshold: enough that fewer than k candidates
+    // (k keys sampled at rate S/n, Poisson) is many standard deviations away
+    const double ks = double(k) * TOPK_SAMPLE / double(n);
+    const int64_t m = int64_t(1.5 * ks + 6.0 * std::sqrt(ks) + 8.0) + 1;
+    topk_sample_kernel<U, KIND><<<1, TOPK_SAMPLE_NT, 0, s>>>(d, n, m, st);
+    topk_filter_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, cand, st);
+    topk_decide_kernel<<<1, 32, 0, s>>>(st, n, k);
+    // level 0: over the candidates, or (fallback) over all keys with the compaction
+    select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(cand, &st->cand_count, 0, st, BITS - 8, SEL_MODE_CAND);
+    select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, nullptr, n, st, BITS - 8, SEL_MODE_FULL);
+    select_pick_kernel<U><<<1, 256, 0, s>>>(st, BITS - 8, LEVELS == 1);
+    select_compact_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, cand, st, out, k, SEL_MODE_FULL);
+    for (int l = 1; l < LEVELS; l++) {
+      const int shift = BITS - 8 * (l + 1);
+      select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(cand, &st->cand_count, 0, st, shift);
+      select_pick_kernel<U><<<1, 256, 0, s>>>(st, shift, l == LEVELS - 1);
+    }
+    topk_gather_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(cand, k, st, out);
     HPCS_CUDA(cudaGetLastError());
   }
   return enqueue_sort<U, KIND, NoValue>(ctx, out, nullptr, k, s);

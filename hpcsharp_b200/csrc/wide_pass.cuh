@@ -68,6 +68,45 @@ __device__ __forceinline__ int wide_src_sel(const WidePlan* plan, int pass) {
   return plan->in_sel[pass - 1] ^ (plan->skip[pass - 1] ? 0 : 1);
 }
 
+// Rank of a key among the earlier keys of its warp with the same digit, on 16-bit counters two
+// to a word: the value an ordered shared atomic returns.  When a digit value is frequent (skewed
+// digits: the top bits of small signed or float keys, low-entropy keys) the lanes of a warp
+// instruction holding the two most frequent values h1, h2 take one atomic per value, made by the
+// lowest of them, and rank among themselves by popcount instead of serialising on one counter;
+// the other lanes rank with their own atomic.  All lanes call it when `grouped` (warp votes).
+__device__ __forceinline__ uint32_t wide_rank(uint32_t* cnt_w, uint32_t d, bool valid, bool grouped, uint32_t h1,
+                                              uint32_t h2, int lane) {
+  if (!grouped) {
+    if (!valid) return 0u;
+    const uint32_t sh = (d & 1u) << 4;
+    return (atomicAdd(cnt_w + (d >> 1), 1u << sh) >> sh) & 0xFFFFu;
+  }
+  const bool is1 = valid && d == h1;
+  const bool is2 = valid && d == h2 && h2 != h1;
+  const uint32_t m1 = __ballot_sync(0xFFFFFFFFu, is1);
+  const uint32_t m2 = __ballot_sync(0xFFFFFFFFu, is2);
+  const int l1 = m1 ? __ffs(m1) - 1 : 0;
+  const int l2 = m2 ? __ffs(m2) - 1 : 0;
+  uint32_t b1 = 0, b2 = 0, r = 0;
+  if (m1 && lane == l1) {
+    const uint32_t sh = (h1 & 1u) << 4;
+    b1 = (atomicAdd(cnt_w + (h1 >> 1), uint32_t(__popc(m1)) << sh) >> sh) & 0xFFFFu;
+  }
+  if (m2 && lane == l2) {
+    const uint32_t sh = (h2 & 1u) << 4;
+    b2 = (atomicAdd(cnt_w + (h2 >> 1), uint32_t(__popc(m2)) << sh) >> sh) & 0xFFFFu;
+  }
+  if (valid && !is1 && !is2) {
+    const uint32_t sh = (d & 1u) << 4;
+    r = (atomicAdd(cnt_w + (d >> 1), 1u << sh) >> sh) & 0xFFFFu;
+  }
+  b1 = __shfl_sync(0xFFFFFFFFu, b1, l1);
+  b2 = __shfl_sync(0xFFFFFFFFu, b2, l2);
+  if (is1) r = b1 + uint32_t(__popc(m1 & lanemask_lt()));
+  if (is2) r = b2 + uint32_t(__popc(m2 & lanemask_lt()));
+  return r;
+}
+
 // ---------------------------------------------------------------------------------------
 // wide_count: CTA j counts digit `pass` of the keys of range j.
 // ---------------------------------------------------------------------------------------
@@ -189,7 +228,8 @@ struct WideSmem {
   static constexpr size_t OFF_RUN = OFF_CNT + size_t(NW) * BINS * 2;  // running start per digit
   static constexpr size_t OFF_GBASE = OFF_RUN + size_t(BINS) * 4;     // this tile's base per digit
   static constexpr size_t OFF_WSUM = OFF_GBASE + size_t(BINS) * 4;
-  static constexpr size_t OFF_MBAR = OFF_WSUM + 32 * 4;
+  static constexpr size_t OFF_TOP = OFF_WSUM + 32 * 4;  // the two most frequent digits
+  static constexpr size_t OFF_MBAR = OFF_TOP + 16;
   static constexpr size_t BYTES = OFF_MBAR + 16;
   static_assert(DPT == 4, "the scan reads four 16-bit counters (8 bytes) per warp and thread");
   static_assert(TILE <= 32768, "tile offsets are 16-bit counters");
@@ -225,6 +265,7 @@ __global__ void __launch_bounds__(NT, 1) wide_pass_kernel(WideArgs args) {
   uint32_t* s_gbase = reinterpret_cast<uint32_t*>(smem + L::OFF_GBASE);
   uint32_t* s_wsum = reinterpret_cast<uint32_t*>(smem + L::OFF_WSUM);
   uint64_t* s_mbar = reinterpret_cast<uint64_t*>(smem + L::OFF_MBAR);
+  unsigned long long* s_top = reinterpret_cast<unsigned long long*>(smem + L::OFF_TOP);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   uint32_t* cnt_w = s_cnt + warp * (BINS / 2);
   const uint16_t* cnt16_w = reinterpret_cast<const uint16_t*>(cnt_w);
@@ -271,7 +312,32 @@ __global__ void __launch_bounds__(NT, 1) wide_pass_kernel(WideArgs args) {
       run += tot[q];
     }
     __syncthreads();
+    // the two most frequent digit values (count, then the lower value, first)
+    unsigned long long best = 0ull;
+#pragma unroll
+    for (int q = 0; q < DPT; q++) {
+      const unsigned long long c = (static_cast<unsigned long long>(tot[q]) << 16) | uint32_t(0xFFFF - (d0 + q));
+      best = c > best ? c : best;
+    }
+    s_top[0] = 0ull;
+    s_top[1] = 0ull;
+    __syncthreads();
+    atomicMax(&s_top[0], best);
+    __syncthreads();
+    best = 0ull;
+#pragma unroll
+    for (int q = 0; q < DPT; q++) {
+      const unsigned long long c = (static_cast<unsigned long long>(tot[q]) << 16) | uint32_t(0xFFFF - (d0 + q));
+      if (c != s_top[0]) best = c > best ? c : best;
+    }
+    atomicMax(&s_top[1], best);
+    __syncthreads();
   }
+  const unsigned long long top1 = s_top[0], top2 = s_top[1];
+  const uint32_t h1 = 0xFFFFu - uint32_t(top1 & 0xFFFFull);
+  const uint32_t h2 = top2 ? 0xFFFFu - uint32_t(top2 & 0xFFFFull) : h1;
+  // one value above 1/16 of the keys: many lanes of an instruction would share its counter
+  const bool grouped = int64_t(top1 >> 16) > args.n / 16;
 
   bool out_of_range = false;
   auto tile_body = [&](auto full_tag, int t) {
@@ -308,13 +374,8 @@ __global__ void __launch_bounds__(NT, 1) wide_pass_kernel(WideArgs args) {
 #pragma unroll
     for (int i = 0; i < KPT; i++) {
       const int idx = wbase + i * 32 + lane;
-      uint32_t r = 0;
-      if (FULL || idx < tile_n) {
-        const uint32_t d = wide_digit<U, KIND>(key[i], shift, mask);
-        const uint32_t sh = (d & 1u) << 4;
-        r = (atomicAdd(cnt_w + (d >> 1), 1u << sh) >> sh) & 0xFFFFu;
-      }
-      rank[i] = r;
+      rank[i] = wide_rank(cnt_w, wide_digit<U, KIND>(key[i], shift, mask), FULL || idx < tile_n, grouped, h1, h2,
+                          lane);
     }
     __syncthreads();  // (A) warp counts complete; the stage buffer is no longer read
 
