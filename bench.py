@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--dtype", default="u32", choices=["u32", "i32", "f32", "u64", "i64", "f64"])
-    ap.add_argument("--scheme", default="auto", choices=["auto", "chunked", "lookback", "wide"],
+    ap.add_argument("--scheme", default="auto", choices=["auto", "chunked", "lookback"],
                     help="plain: the digit-pass scheme of the library (auto picks by key type and n)")
     ap.add_argument("--slots", type=int, default=4, help="distinct input copies cycled through")
     ap.add_argument("--e2e-steps", type=int, default=0, help="0 = same as --steps (capped at 20)")

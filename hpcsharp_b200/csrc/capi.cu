@@ -144,9 +144,9 @@ int probe_rank_order(hpcs_ctx* ctx, int* ordered) {
 int check_device_errors(hpcs_ctx* ctx);
 
 // ---- probe of the shipping pass kernels ---------------------------------------------------
-// Keys whose digits (11-bit, so also every 8-bit digit) take few values, so many lanes of a warp
-// instruction share a counter: `values` = 20 keeps them below the grouped-ranking threshold, 3
-// sends the frequent values to the grouped ranking; items are the input positions.
+// Keys whose digits take few values, so many lanes of a warp instruction share a counter: with
+// `values` = 20 every byte digit has at most 20 values, with 3 at most 3; items are the input
+// positions.
 __global__ void probe_fill_kernel(uint32_t* keys, uint32_t* items, int64_t n, uint32_t values) {
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -154,8 +154,9 @@ __global__ void probe_fill_kernel(uint32_t* keys, uint32_t* items, int64_t n, ui
     x ^= x >> 15;
     x *= 0x2C1B3C6Du;
     x ^= x >> 12;
-    const uint32_t d0 = (x & 0xFFFFu) % values, d1 = (x >> 16) % values, d2 = (x * 0x27D4EB2Fu >> 8) % values;
-    keys[i] = d0 | (d1 << 11) | (d2 << 22);
+    const uint32_t y = x * 0x27D4EB2Fu;
+    keys[i] = ((x & 0xFFFFu) % values) | (((x >> 16) % values) << 8) | (((y >> 8) % values) << 16) |
+              (((y >> 20) % values) << 24);
     if (items) items[i] = uint32_t(i);
   }
 }
@@ -171,7 +172,7 @@ __global__ void probe_check_kernel(const uint32_t* keys, const uint32_t* items, 
   if (v) atomicAdd(bad, v);
 }
 
-// Runs the shipping ordered-atomic pass kernels -- the wide passes and the chunked 8-bit passes,
+// Runs the shipping ordered-atomic pass kernels -- the chunked passes and the look-back passes,
 // keys only and with items -- on inputs with many equal digits per warp instruction and checks
 // the results for order and stability.  Any violation sends the context to the peer-mask
 // ranking, which is defined by PTX.  The same code generation and occupancy as a real sort: the
@@ -188,7 +189,7 @@ int probe_shipping_kernels(hpcs_ctx* ctx, int* ok) {
   const int saved_scheme = ctx->cfg.pass_scheme;
   ctx->rank_mode = RANK_ORDERED_ATOMIC;
   cudaStream_t s = ctx->stream;
-  for (int scheme : {int(HPCS_PASSES_WIDE), int(HPCS_PASSES_CHUNKED)}) {
+  for (int scheme : {int(HPCS_PASSES_CHUNKED), int(HPCS_PASSES_LOOKBACK)}) {
     ctx->cfg.pass_scheme = scheme;
     for (uint32_t values : {20u, 3u}) {
       for (int with_items = 0; with_items < 2 && rc == HPCS_OK; with_items++) {

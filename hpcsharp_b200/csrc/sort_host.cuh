@@ -11,7 +11,6 @@
 
 #include "../../include/hpcs_gpu.h"
 #include "chunk_pass.cuh"
-#include "wide_pass.cuh"
 #include "radix_kernels.cuh"
 
 namespace hpcs {
@@ -332,122 +331,6 @@ inline ChunkGeometry chunk_geometry(int64_t n, int tile, int max_ranges) {
 
 // Enqueue a full LSD sort of n keys (and optional 4-byte items) in device memory.
 // keys/vals are sorted in place (with scratch B owned by the context).
-// ---- wide-digit passes (wide_pass.cuh) ---------------------------------------------------
-// Tile shapes of the wide pass (threads x keys per thread), 32-bit keys only.
-template <class V>
-struct WideConfig;
-template <>
-struct WideConfig<NoValue> {
-  static constexpr int NT = 512, KPT = 32;
-};
-template <>
-struct WideConfig<uint32_t> {
-  static constexpr int NT = 512, KPT = 16;
-};
-// The automatic scheme takes the wide passes for 32-bit keys from this many keys on (below it
-// the per-range count tables and the extra count read do not pay off).
-constexpr int64_t WIDE_MIN_KEYS = int64_t(32) << 20;
-
-// Digits of a 32-bit key: bits [0,11), [11,22), [22,32).
-constexpr int WIDE32_PASSES = 3;
-constexpr int WIDE32_SHIFT[WIDE32_PASSES] = {0, 11, 22};
-constexpr int WIDE32_BITS[WIDE32_PASSES] = {11, 11, 10};
-
-template <class U, int KIND, class V>
-int enqueue_sort_wide(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t s) {
-  static_assert(sizeof(U) == 4, "wide passes: 32-bit keys");
-  using C = WideConfig<V>;
-  using L = WideSmem<U, V, C::NT, C::KPT>;
-  constexpr bool PAIRS = !std::is_same<V, NoValue>::value;
-  const int64_t tiles = (n + L::TILE - 1) / L::TILE;
-  const int64_t per = (tiles + ctx->sms - 1) / ctx->sms;  // tiles per range
-  const int J = int((tiles + per - 1) / per);
-  const uint32_t range_keys = uint32_t(per * L::TILE);
-  U* a = keys;
-  uint32_t* va = vals;
-  const bool keys_unaligned = (reinterpret_cast<uintptr_t>(keys) & 15) != 0;
-  const bool vals_unaligned = PAIRS && (reinterpret_cast<uintptr_t>(vals) & 15) != 0;
-  int rc;
-  if ((rc = ensure(ctx, ctx->keys_b, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
-  if (PAIRS && (rc = ensure(ctx, ctx->vals_b, size_t(n) * 4)) != HPCS_OK) return rc;
-  if (keys_unaligned) {
-    if ((rc = ensure(ctx, ctx->keys_a, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
-    a = static_cast<U*>(ctx->keys_a.ptr);
-    HPCS_CUDA(cudaMemcpyAsync(a, keys, size_t(n) * sizeof(U), cudaMemcpyDeviceToDevice, s));
-  }
-  if (vals_unaligned) {
-    if ((rc = ensure(ctx, ctx->vals_a, size_t(n) * 4)) != HPCS_OK) return rc;
-    va = static_cast<uint32_t*>(ctx->vals_a.ptr);
-    HPCS_CUDA(cudaMemcpyAsync(va, vals, size_t(n) * 4, cudaMemcpyDeviceToDevice, s));
-  }
-  const size_t table = size_t(J) * WIDE_MAX_BINS;
-  if ((rc = ensure(ctx, ctx->status0, (2 * table + WIDE_MAX_BINS) * 4)) != HPCS_OK) return rc;
-  if ((rc = ensure(ctx, ctx->plan, sizeof(SortPlan) > sizeof(WidePlan) ? sizeof(SortPlan) : sizeof(WidePlan))) !=
-      HPCS_OK)
-    return rc;
-  WideArgs args{};
-  args.keys_a = a;
-  args.keys_b = ctx->keys_b.ptr;
-  args.vals_a = va;
-  args.vals_b = PAIRS ? ctx->vals_b.ptr : nullptr;
-  args.n = n;
-  args.plan = static_cast<WidePlan*>(ctx->plan.ptr);
-  args.rcount = static_cast<uint32_t*>(ctx->status0.ptr);
-  args.rprefix = args.rcount + table;
-  args.totals = args.rprefix + table;
-  args.ranges = J;
-  args.range_keys = range_keys;
-  args.spin_limit_ns = uint64_t(ctx->cfg.spin_limit_ns);
-  auto kc = wide_count_kernel<U, KIND>;
-  auto kp = wide_pass_kernel<U, KIND, V, C::NT, C::KPT>;
-  static int attr_set[64] = {0};
-  if (!attr_set[ctx->device & 63]) {
-    HPCS_CUDA(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(WIDE_COUNT_SMEM)));
-    HPCS_CUDA(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, int(L::BYTES)));
-    attr_set[ctx->device & 63] = 1;
-  }
-  HPCS_CUDA(cudaMemsetAsync(args.plan, 0, sizeof(WidePlan), s));
-  for (int p = 0; p < WIDE32_PASSES; p++) {
-    args.pass = p;
-    args.shift = WIDE32_SHIFT[p];
-    args.bits = WIDE32_BITS[p];
-    {
-      KernelTimer kt(ctx, s, HPCS_K_HISTOGRAM);
-      kc<<<J, WIDE_COUNT_NT, WIDE_COUNT_SMEM, s>>>(args);
-      HPCS_CUDA(cudaGetLastError());
-      wide_plan_kernel<<<(1 << args.bits) / 32, WIDE_PLAN_NT, 0, s>>>(args);
-      HPCS_CUDA(cudaGetLastError());
-    }
-    {
-      KernelTimer kt(ctx, s, HPCS_K_ONESWEEP);
-      kp<<<J, C::NT, L::BYTES, s>>>(args);
-      HPCS_CUDA(cudaGetLastError());
-    }
-  }
-  {
-    const int64_t want = (n + 255) / 256;
-    const int grid = int(want > int64_t(ctx->sms) * 8 ? int64_t(ctx->sms) * 8 : want);
-    KernelTimer kt(ctx, s, HPCS_K_FINALIZE);
-    wide_finalize_kernel<U><<<grid, 256, 0, s>>>(args, WIDE32_PASSES, PAIRS ? 1 : 0, device_error_word(ctx));
-    HPCS_CUDA(cudaGetLastError());
-  }
-  if (keys_unaligned)
-    HPCS_CUDA(cudaMemcpyAsync(keys, a, size_t(n) * sizeof(U), cudaMemcpyDeviceToDevice, s));
-  if (vals_unaligned) HPCS_CUDA(cudaMemcpyAsync(vals, va, size_t(n) * 4, cudaMemcpyDeviceToDevice, s));
-  return HPCS_OK;
-}
-
-// Whether a sort of n keys runs on the wide passes: 32-bit keys, the ordered-atomic ranking,
-// forced by HPCS_PASSES_WIDE or chosen by the automatic scheme for large sorts on the context's
-// own scratch.
-template <class U, int KIND>
-inline bool use_wide_passes(hpcs_ctx* ctx, int64_t n) {
-  if (sizeof(U) != 4 || ctx->rank_mode != RANK_ORDERED_ATOMIC) return false;
-  if (ctx->cfg.pass_scheme == HPCS_PASSES_WIDE) return true;
-  return ctx->cfg.pass_scheme == HPCS_PASSES_AUTO && KIND == KIND_UNSIGNED && n >= WIDE_MIN_KEYS &&
-         !ctx->status0.borrowed;
-}
-
 template <class U, int KIND, class V>
 int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t s) {
   using CA = SortConfig<U, V, RANK_ORDERED_ATOMIC>;
@@ -455,9 +338,6 @@ int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t
   constexpr bool PAIRS = !std::is_same<V, NoValue>::value;
   if (n <= 1) return HPCS_OK;
   if (n > MAX_KEYS_PER_SORT) return fail(HPCS_ERR_RANGE, "n exceeds HPCS_MAX_KEYS");
-  if constexpr (sizeof(U) == 4) {
-    if (use_wide_passes<U, KIND>(ctx, n)) return enqueue_sort_wide<U, KIND, V>(ctx, keys, vals, n, s);
-  }
   if (ctx->cfg.pass_scheme == HPCS_PASSES_LOOKBACK && n > MAX_KEYS_LOOKBACK)
     return fail(HPCS_ERR_RANGE, "look-back passes take at most 2^30 - 1 keys (30-bit prefixes)");
   const bool lookback = ctx->cfg.pass_scheme == HPCS_PASSES_LOOKBACK ||

@@ -79,7 +79,7 @@ class HpcsConfig(C.Structure):
     ]
 
 
-PASS_SCHEMES = {"auto": 0, "lookback": 1, "chunked": 2, "wide": 3}
+PASS_SCHEMES = {"auto": 0, "lookback": 1, "chunked": 2}
 KCLASS = {"histogram": 0, "onesweep": 1, "finalize": 2, "topk": 3, "segmented": 4, "shard": 5, "lookback": 6}
 
 

@@ -69,7 +69,7 @@ typedef enum hpcs_dtype {
 typedef struct hpcs_ctx hpcs_ctx;
 
 /* Digit-pass schemes (hpcs_config.pass_scheme). */
-enum { HPCS_PASSES_AUTO = 0, HPCS_PASSES_LOOKBACK = 1, HPCS_PASSES_CHUNKED = 2, HPCS_PASSES_WIDE = 3 };
+enum { HPCS_PASSES_AUTO = 0, HPCS_PASSES_LOOKBACK = 1, HPCS_PASSES_CHUNKED = 2 };
 
 typedef struct hpcs_config {
   int64_t pool_bytes;          /* device scratch budget of the context; 0 = unlimited */
@@ -82,9 +82,7 @@ typedef struct hpcs_config {
   int32_t pass_scheme;         /* digit passes: HPCS_PASSES_AUTO (0, default) picks by key
                                   type and n; HPCS_PASSES_LOOKBACK (1): single-pass decoupled
                                   look-back; HPCS_PASSES_CHUNKED (2): per-range counts from
-                                  the previous pass, no inter-CTA waiting; HPCS_PASSES_WIDE (3):
-                                  32-bit keys in three passes of up to 11-bit digits, each after
-                                  a counting read of its input (other keys: as AUTO) */
+                                  the previous pass, no inter-CTA waiting */
   int32_t staged_host_copies;  /* host-array calls on pageable memory (default 1): copy through
                                   the context's pinned buffers in chunks, several host threads
                                   copying while the DMA engine moves earlier chunks; 0: one
