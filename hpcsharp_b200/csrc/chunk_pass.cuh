@@ -53,8 +53,10 @@ struct ChunkSmem {
   static constexpr size_t OFF_MSK = OFF_CNT + size_t(NW) * RS * 4;
   static constexpr size_t MSK_BYTES = MODE == RANK_PEER_MASK ? size_t(NW) * 2 * RADIX * 4 : 0;
   static constexpr size_t OFF_RUN = (OFF_MSK + MSK_BYTES + 15) / 16 * 16;  // running start per digit
-  static constexpr size_t OFF_GBASE = OFF_RUN + RADIX * 4;                // this tile's base per digit
-  static constexpr size_t OFF_WSUM = OFF_GBASE + RADIX * 4;
+  // per digit for this tile: {global base, next-digit counter row of its first key's range,
+  // first position of the following range, 0}
+  static constexpr size_t OFF_META = OFF_RUN + RADIX * 4;
+  static constexpr size_t OFF_WSUM = OFF_META + RADIX * 16;
   static constexpr size_t OFF_MBAR = (OFF_WSUM + 32 * 4 + 7) / 8 * 8;
   static constexpr size_t OFF_CTAB = (OFF_MBAR + 16 + 15) / 16 * 16;  // [J][128] words
   static constexpr size_t BASE_BYTES = OFF_CTAB;
@@ -117,7 +119,7 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
   uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + L::OFF_CNT);
   uint32_t* s_msk = reinterpret_cast<uint32_t*>(smem + L::OFF_MSK);
   uint32_t* s_run = reinterpret_cast<uint32_t*>(smem + L::OFF_RUN);
-  uint32_t* s_gbase = reinterpret_cast<uint32_t*>(smem + L::OFF_GBASE);
+  uint4* s_meta = reinterpret_cast<uint4*>(smem + L::OFF_META);
   uint32_t* s_wsum = reinterpret_cast<uint32_t*>(smem + L::OFF_WSUM);
   uint64_t* s_mbar = reinterpret_cast<uint64_t*>(smem + L::OFF_MBAR);
   uint32_t* s_ctab = reinterpret_cast<uint32_t*>(smem + L::OFF_CTAB);
@@ -301,8 +303,12 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
         run += c[m];
       }
       if (sq == 0) {
+        // r: global position of this tile's first key of digit sd.  The digit's keys of the tile
+        // (at most one tile, and a range holds whole tiles) fall in r's range q or the next one.
         const uint32_t r = s_run[sd];
-        s_gbase[sd] = r - local;
+        uint32_t q = __umulhi(r, magic);
+        q -= (q * LK > r) ? 1u : 0u;
+        s_meta[sd] = make_uint4(r - local, q * (RADIX / 2), (q + 1u) * LK, 0u);
         s_run[sd] = r + total;
       }
     }
@@ -346,15 +352,15 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
         const U k = key[i];
         const uint32_t d = dig(k);
         if (PAIRS) dsave[i] = uint8_t(d);
-        const uint32_t pos = s_gbase[d] + uint32_t(s);
+        const uint4 m = s_meta[d];
+        const uint32_t pos = m.x + uint32_t(s);
         if (pos < n32) {
           kout_base[pos] = k;
           const uint32_t e = ndig(k);
           if (nshift >= 0 && !next_skewed && e != next_heavy) {
-            uint32_t r = __umulhi(pos, magic);
-            r -= (r * LK > pos) ? 1u : 0u;
+            const uint32_t row = m.y + (pos >= m.z ? uint32_t(RADIX / 2) : 0u);
             const uint32_t inc = 1u + (e & 1u) * 0xFFFFu;
-            const uint32_t old = atomicAdd(s_ctab + r * (RADIX / 2) + (e >> 1), inc);
+            const uint32_t old = atomicAdd(s_ctab + row + (e >> 1), inc);
             // a half went from 0x7FFF to 0x8000 (the other half is unchanged)
             if ((old + inc) & ~old & 0x80008000u) crossed |= 1u << i;
           }
@@ -369,11 +375,11 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
         const int s = i * NT + tid;
         const U k = key[i];
         const uint32_t e = ndig(k);
-        const uint32_t pos = s_gbase[dig(k)] + uint32_t(s);
-        uint32_t r = __umulhi(pos, magic);
-        r -= (r * LK > pos) ? 1u : 0u;
+        const uint4 m = s_meta[dig(k)];
+        const uint32_t pos = m.x + uint32_t(s);
+        const uint32_t row = m.y + (pos >= m.z ? uint32_t(RADIX / 2) : 0u);
         const bool counted = (FULL || s < tile_n) && pos < n32 && e != next_heavy;
-        const uint32_t word = r * (RADIX / 2) + (e >> 1);
+        const uint32_t word = row + (e >> 1);
         const uint32_t unit = 1u + (e & 1u) * 0xFFFFu;
         const uint32_t code = (word << 1) | (e & 1u);
         const uint32_t lanes = __ballot_sync(0xFFFFFFFFu, counted);
@@ -396,13 +402,13 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
         if ((crossed >> i) & 1u) {
           const int s = i * NT + tid;
           const U k = key[i];
-          const uint32_t pos = s_gbase[dig(k)] + uint32_t(s);
+          const uint4 m = s_meta[dig(k)];
+          const uint32_t pos = m.x + uint32_t(s);
+          const uint32_t row = m.y + (pos >= m.z ? uint32_t(RADIX / 2) : 0u);
           const uint32_t e = ndig(k);
-          uint32_t r = __umulhi(pos, magic);
-          r -= (r * LK > pos) ? 1u : 0u;
           const uint32_t sh = (e & 1u) << 4;
-          atomicSub(s_ctab + r * (RADIX / 2) + (e >> 1), 0x8000u << sh);
-          atomicAdd(cout + r * RADIX + e, 0x8000u);
+          atomicSub(s_ctab + row + (e >> 1), 0x8000u << sh);
+          atomicAdd(cout + 2u * row + e, 0x8000u);
         }
       }
     }
@@ -428,7 +434,7 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
       for (int i = 0; i < KPT; i++) {
         const int s = i * NT + tid;
         if (FULL || s < tile_n) {
-          const uint32_t pos = s_gbase[dsave[i]] + uint32_t(s);
+          const uint32_t pos = s_meta[dsave[i]].x + uint32_t(s);
           if (pos < n32) vout[pos] = sv[s];
         }
       }

@@ -60,7 +60,7 @@ class CopyPool {
 
  private:
   void piece(int idx) {
-    const size_t per = (bytes_ / size_t(parts()) + 63) & ~size_t(63);
+    const size_t per = ((bytes_ + size_t(parts()) - 1) / size_t(parts()) + 63) & ~size_t(63);  // covers bytes_
     const size_t lo = std::min(bytes_, per * size_t(idx));
     const size_t hi = std::min(bytes_, lo + per);
     if (hi > lo) std::memcpy(dst_ + lo, src_ + lo, hi - lo);

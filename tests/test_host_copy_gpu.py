@@ -19,7 +19,10 @@ def plain_ctx():
     c.close()
 
 
-@pytest.mark.parametrize("n", [2 * CHUNK_KEYS, 2 * CHUNK_KEYS + 1, 5 * CHUNK_KEYS - 3, 9 * CHUNK_KEYS + 12345])
+# sizes whose last chunk is empty, tiny, just under a chunk, and over 1 MiB but not a multiple of the
+# copy threads' 64-byte pieces (every byte of every chunk must be copied)
+@pytest.mark.parametrize("n", [2 * CHUNK_KEYS, 2 * CHUNK_KEYS + 1, 5 * CHUNK_KEYS - 3, 9 * CHUNK_KEYS + 12345,
+                               3 * CHUNK_KEYS + 3_222_785])
 def test_staged_sort_matches_plain_copy_and_oracle(ctx, plain_ctx, orc, n):
     a = datagen.u32_uniform(n, seed=n % 1000)
     staged = a.copy()
@@ -41,6 +44,15 @@ def test_staged_pairs_and_u64(ctx, orc):
     ctx.sort_pairs(keys, items)
     np.testing.assert_array_equal(keys, k2)
     np.testing.assert_array_equal(items, i2)
+
+
+def test_staged_16_bit_counting_sort(ctx):
+    """A 16-bit array whose byte count is not a multiple of 4 (odd n): the last chunk's last bytes."""
+    n = 40_000_001
+    a = np.random.default_rng(3).integers(0, 1 << 16, size=n, dtype=np.int64).astype(np.uint16)
+    got = a.copy()
+    ctx.sort(got)
+    np.testing.assert_array_equal(got, np.sort(a))
 
 
 def test_pinned_host_array_is_not_staged(ctx, orc):
