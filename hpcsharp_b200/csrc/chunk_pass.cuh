@@ -53,10 +53,10 @@ struct ChunkSmem {
   static constexpr size_t OFF_MSK = OFF_CNT + size_t(NW) * RS * 4;
   static constexpr size_t MSK_BYTES = MODE == RANK_PEER_MASK ? size_t(NW) * 2 * RADIX * 4 : 0;
   static constexpr size_t OFF_RUN = (OFF_MSK + MSK_BYTES + 15) / 16 * 16;  // running start per digit
-  // per digit for this tile: {global base; next-digit counter row of its first key's range in
-  // the low 16 bits, and in the high 16 bits the first tile position in the following range}
+  // per digit for this tile: {global base, next-digit counter row of its first key's range,
+  // first position of the following range, 0}
   static constexpr size_t OFF_META = OFF_RUN + RADIX * 4;
-  static constexpr size_t OFF_WSUM = OFF_META + RADIX * 8;
+  static constexpr size_t OFF_WSUM = OFF_META + RADIX * 16;
   static constexpr size_t OFF_MBAR = (OFF_WSUM + 32 * 4 + 7) / 8 * 8;
   static constexpr size_t OFF_CTAB = (OFF_MBAR + 16 + 15) / 16 * 16;  // [J][128] words
   static constexpr size_t BASE_BYTES = OFF_CTAB;
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
   uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + L::OFF_CNT);
   uint32_t* s_msk = reinterpret_cast<uint32_t*>(smem + L::OFF_MSK);
   uint32_t* s_run = reinterpret_cast<uint32_t*>(smem + L::OFF_RUN);
-  uint2* s_meta = reinterpret_cast<uint2*>(smem + L::OFF_META);
+  uint4* s_meta = reinterpret_cast<uint4*>(smem + L::OFF_META);
   uint32_t* s_wsum = reinterpret_cast<uint32_t*>(smem + L::OFF_WSUM);
   uint64_t* s_mbar = reinterpret_cast<uint64_t*>(smem + L::OFF_MBAR);
   uint32_t* s_ctab = reinterpret_cast<uint32_t*>(smem + L::OFF_CTAB);
@@ -308,11 +308,7 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
         const uint32_t r = s_run[sd];
         uint32_t q = __umulhi(r, magic);
         q -= (q * LK > r) ? 1u : 0u;
-        const uint32_t gbase = r - local;
-        // tile positions s of digit sd run from local; the range changes at (q + 1) * LK - gbase
-        const uint32_t to_next = (q + 1u) * LK - r;  // keys of the digit still in range q
-        const uint32_t split = to_next >= uint32_t(TILE) ? 0xFFFFu : local + to_next;
-        s_meta[sd] = make_uint2(gbase, q * (RADIX / 2) | (split << 16));
+        s_meta[sd] = make_uint4(r - local, q * (RADIX / 2), (q + 1u) * LK, 0u);
         s_run[sd] = r + total;
       }
     }
@@ -356,13 +352,13 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
         const U k = key[i];
         const uint32_t d = dig(k);
         if (PAIRS) dsave[i] = uint8_t(d);
-        const uint2 m = s_meta[d];
+        const uint4 m = s_meta[d];
         const uint32_t pos = m.x + uint32_t(s);
         if (pos < n32) {
           kout_base[pos] = k;
           const uint32_t e = ndig(k);
           if (nshift >= 0 && !next_skewed && e != next_heavy) {
-            const uint32_t row = (m.y & 0xFFFFu) + (uint32_t(s) >= (m.y >> 16) ? uint32_t(RADIX / 2) : 0u);
+            const uint32_t row = m.y + (pos >= m.z ? uint32_t(RADIX / 2) : 0u);
             const uint32_t inc = 1u + (e & 1u) * 0xFFFFu;
             const uint32_t old = atomicAdd(s_ctab + row + (e >> 1), inc);
             // a half went from 0x7FFF to 0x8000 (the other half is unchanged)
@@ -379,9 +375,9 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
         const int s = i * NT + tid;
         const U k = key[i];
         const uint32_t e = ndig(k);
-        const uint2 m = s_meta[dig(k)];
+        const uint4 m = s_meta[dig(k)];
         const uint32_t pos = m.x + uint32_t(s);
-        const uint32_t row = (m.y & 0xFFFFu) + (uint32_t(s) >= (m.y >> 16) ? uint32_t(RADIX / 2) : 0u);
+        const uint32_t row = m.y + (pos >= m.z ? uint32_t(RADIX / 2) : 0u);
         const bool counted = (FULL || s < tile_n) && pos < n32 && e != next_heavy;
         const uint32_t word = row + (e >> 1);
         const uint32_t unit = 1u + (e & 1u) * 0xFFFFu;
@@ -406,9 +402,9 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
         if ((crossed >> i) & 1u) {
           const int s = i * NT + tid;
           const U k = key[i];
-          const uint2 m = s_meta[dig(k)];
+          const uint4 m = s_meta[dig(k)];
           const uint32_t pos = m.x + uint32_t(s);
-          const uint32_t row = (m.y & 0xFFFFu) + (uint32_t(s) >= (m.y >> 16) ? uint32_t(RADIX / 2) : 0u);
+          const uint32_t row = m.y + (pos >= m.z ? uint32_t(RADIX / 2) : 0u);
           const uint32_t e = ndig(k);
           const uint32_t sh = (e & 1u) << 4;
           atomicSub(s_ctab + row + (e >> 1), 0x8000u << sh);
