@@ -776,6 +776,12 @@ int hpcs_ctx_destroy(hpcs_ctx* ctx) {
     if (ctx->seg_join[b]) cudaEventDestroy(ctx->seg_join[b]);
   }
   if (ctx->seg_fork) cudaEventDestroy(ctx->seg_fork);
+  if (ctx->seg_grid_stream) {
+    cudaStreamSynchronize(ctx->seg_grid_stream);
+    cudaStreamDestroy(ctx->seg_grid_stream);
+  }
+  if (ctx->seg_grid_fork) cudaEventDestroy(ctx->seg_grid_fork);
+  if (ctx->seg_grid_join) cudaEventDestroy(ctx->seg_grid_join);
   delete ctx->stager;
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;

@@ -71,7 +71,7 @@ struct ChunkSmem {
 // [q * NWG, (q + 1) * NWG), q = t % G.  With the row stride RS = 256 + 32 / NW the NWG x 32
 // counters a warp instruction reads fall in 32 distinct banks.
 template <class U, int KIND, class V, int NT, int KPT, int MODE>
-__global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
+__device__ __forceinline__ void chunk_pass_body(const SortArgs& args, const int j) {
   using L = ChunkSmem<U, V, NT, KPT, MODE>;
   using KO = KeyOrder<U, KIND>;
   constexpr bool PAIRS = L::PAIRS;
@@ -95,7 +95,6 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
   uint32_t* err = const_cast<uint32_t*>(&plan->error);
   const uint32_t n32 = uint32_t(args.n);
   const int J = args.chunks;
-  const int j = blockIdx.x;
   const uint32_t LK = args.chunk_keys;
   const uint32_t magic = args.chunk_magic;
   const int64_t clo = int64_t(j) * LK;
@@ -464,6 +463,23 @@ __global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
       if (v >> 16) atomicAdd(cout + 2 * i + 1, v >> 16);
     }
   }
+}
+
+// One digit pass of one array: CTA j owns range j.
+template <class U, int KIND, class V, int NT, int KPT, int MODE>
+__global__ void __launch_bounds__(NT, 1) chunk_pass_kernel(SortArgs args) {
+  chunk_pass_body<U, KIND, V, NT, KPT, MODE>(args, int(blockIdx.x));
+}
+
+// One digit pass of many arrays in one launch (the batched sort's grid-level path): CTA c owns
+// range map[c].y of array map[c].x, whose sort arguments are args[map[c].x].
+template <class U, int KIND, class V, int NT, int KPT, int MODE>
+__global__ void __launch_bounds__(NT, 1) seg_chunk_pass_kernel(const SortArgs* __restrict__ args,
+                                                               const int2* __restrict__ map, int pass) {
+  const int2 m = map[blockIdx.x];
+  SortArgs a = args[m.x];
+  a.pass = pass;
+  chunk_pass_body<U, KIND, V, NT, KPT, MODE>(a, m.y);
 }
 
 }  // namespace hpcs

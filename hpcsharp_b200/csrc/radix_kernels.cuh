@@ -123,10 +123,12 @@ struct HistSmem {
   static constexpr size_t BYTES = size_t(P) * RADIX * COPIES * 4;
 };
 
+// cta / ncta: this CTA's index and the CTA count of this array's histogram (the grid of a
+// single-array launch; the array's ranges in the batched sort's grid-level launch).
 template <class U, int KIND, int NT>
-__global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restrict__ keys, int64_t n,
-                                                                 uint32_t* __restrict__ hist_out,
-                                                                 SortArgs args, int make_plan) {
+__device__ __forceinline__ void hist_all_digits_body(const U* __restrict__ keys, int64_t n,
+                                                     uint32_t* __restrict__ hist_out, const SortArgs& args,
+                                                     int make_plan, const int cta, const int ncta) {
   constexpr int P = HistSmem<U>::P;
   constexpr int COPIES = HistSmem<U>::COPIES;
   constexpr int VEC = 16 / int(sizeof(U));
@@ -152,11 +154,11 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
   const bool chunked = args.chunk_hist != nullptr;
   const int64_t nvec = n / VEC;
   const uint4* vkeys = reinterpret_cast<const uint4*>(keys);
-  int64_t vend = nvec, stride = int64_t(gridDim.x) * NT;
-  int64_t i = int64_t(blockIdx.x) * NT + tid;
-  bool owns_tail = blockIdx.x == 0;
+  int64_t vend = nvec, stride = int64_t(ncta) * NT;
+  int64_t i = int64_t(cta) * NT + tid;
+  bool owns_tail = cta == 0;
   if (chunked) {
-    const int64_t lo = int64_t(blockIdx.x) * args.chunk_keys;  // a multiple of VEC
+    const int64_t lo = int64_t(cta) * args.chunk_keys;  // a multiple of VEC
     const int64_t hi = lo + args.chunk_keys < n ? lo + args.chunk_keys : n;
     i = lo / VEC + tid;
     vend = hi / VEC;
@@ -189,7 +191,7 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
   __syncthreads();
   // fold the copies (rotated start so a warp's reads hit distinct banks) into the output,
   // and (chunked) into this range's row of per-range counts
-  uint32_t* crow = chunked ? args.chunk_hist + int64_t(blockIdx.x) * P * RADIX : nullptr;
+  uint32_t* crow = chunked ? args.chunk_hist + int64_t(cta) * P * RADIX : nullptr;
   for (int j = tid; j < P * RADIX; j += NT) {
     uint32_t c = 0;
 #pragma unroll 8
@@ -202,19 +204,19 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
 
   if (chunked) {
     // the first executed pass adds its next-digit counts into table 1
-    uint32_t* t1 = args.ctab + (int64_t(args.chunks) + blockIdx.x) * RADIX;
+    uint32_t* t1 = args.ctab + (int64_t(args.chunks) + cta) * RADIX;
     for (int j = tid; j < RADIX; j += NT) t1[j] = 0;
   } else {
     // Zero the first look-back buffer for the first executed pass.
     uint32_t* s0 = args.status[0];
     const int64_t words = int64_t(args.num_tiles) * RADIX;
-    const int64_t gstride = int64_t(gridDim.x) * NT;
-    for (int64_t w = int64_t(blockIdx.x) * NT + tid; w < words; w += gstride) s0[w] = 0;
+    const int64_t gstride = int64_t(ncta) * NT;
+    for (int64_t w = int64_t(cta) * NT + tid; w < words; w += gstride) s0[w] = 0;
   }
   // Last-block-done: the final CTA builds the plan.
   __threadfence();
   __syncthreads();
-  if (tid == 0) s_last = (atomicAdd(&args.plan->done_blocks, 1u) == gridDim.x - 1) ? 1u : 0u;
+  if (tid == 0) s_last = (atomicAdd(&args.plan->done_blocks, 1u) == uint32_t(ncta) - 1u) ? 1u : 0u;
   __syncthreads();
   if (!s_last) return;
   __threadfence();
@@ -299,6 +301,23 @@ __global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restr
     plan->use_lookback = lb;
     __threadfence();
   }
+}
+
+template <class U, int KIND, int NT>
+__global__ void __launch_bounds__(NT, 1) hist_all_digits_kernel(const U* __restrict__ keys, int64_t n,
+                                                                 uint32_t* __restrict__ hist_out,
+                                                                 SortArgs args, int make_plan) {
+  hist_all_digits_body<U, KIND, NT>(keys, n, hist_out, args, make_plan, int(blockIdx.x), int(gridDim.x));
+}
+
+// The fused histogram (and plan) of many arrays in one launch (the batched sort's grid-level
+// path): CTA c counts range map[c].y of array map[c].x, whose sort arguments are args[map[c].x].
+template <class U, int KIND, int NT>
+__global__ void __launch_bounds__(NT, 1) seg_hist_all_digits_kernel(const SortArgs* __restrict__ args,
+                                                                    const int2* __restrict__ map) {
+  const int2 m = map[blockIdx.x];
+  const SortArgs a = args[m.x];
+  hist_all_digits_body<U, KIND, NT>(static_cast<const U*>(a.keys_a), a.n, &a.plan->hist[0][0], a, 1, m.y, a.chunks);
 }
 
 // =====================================================================================
@@ -813,6 +832,26 @@ __global__ void finalize_kernel(SortArgs args, int has_vals, uint32_t* err_accum
     uint32_t* vd = static_cast<uint32_t*>(args.vals_a);
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) vd[i] = vs[i];
   }
+}
+
+// The batched sort's grid-level path: CTA c copies range map[c].y of array map[c].x back into
+// the caller's buffer when that array's result ended in its scratch buffer (an odd number of
+// passes ran), and the array's first CTA folds its device error bits into the context's word.
+template <class U>
+__global__ void seg_finalize_kernel(const SortArgs* __restrict__ args, const int2* __restrict__ map,
+                                    uint32_t* err_accum) {
+  const int2 m = map[blockIdx.x];
+  const SortArgs a = args[m.x];
+  if (m.y == 0 && threadIdx.x == 0) {
+    const uint32_t e = ld_volatile(&a.plan->error);
+    if (e) atomicOr(err_accum, e);
+  }
+  if (a.plan->final_sel != 1) return;
+  const int64_t lo = int64_t(m.y) * a.chunk_keys;
+  const int64_t hi = lo + a.chunk_keys < a.n ? lo + a.chunk_keys : a.n;
+  const U* src = static_cast<const U*>(a.keys_b);
+  U* dst = static_cast<U*>(a.keys_a);
+  for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) dst[i] = src[i];
 }
 
 }  // namespace hpcs

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "../../include/hpcs_gpu.h"
+#include "seg_grid.cuh"
 #include "segmented_host.cuh"
 
 struct hpcs_segplan {
@@ -16,6 +17,7 @@ struct hpcs_segplan {
   uint32_t* d_queue = nullptr;
   void* d_scratch = nullptr;
   size_t scratch_bytes = 0;
+  void* d_grid = nullptr;  // grid-level path: per-array sort arguments and the CTA map
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t capture_stream = nullptr;
@@ -52,6 +54,9 @@ struct DeviceGuard2 {
 
 int ensure_seg_streams(hpcs_ctx* ctx) {
   if (ctx->seg_fork) return HPCS_OK;
+  HPCS_CUDA(cudaStreamCreateWithFlags(&ctx->seg_grid_stream, cudaStreamNonBlocking));
+  HPCS_CUDA(cudaEventCreateWithFlags(&ctx->seg_grid_fork, cudaEventDisableTiming));
+  HPCS_CUDA(cudaEventCreateWithFlags(&ctx->seg_grid_join, cudaEventDisableTiming));
   for (int b = 0; b < hpcs_ctx::SEG_BRANCHES; b++) {
     HPCS_CUDA(cudaStreamCreateWithFlags(&ctx->seg_streams[b], cudaStreamNonBlocking));
     HPCS_CUDA(cudaEventCreateWithFlags(&ctx->seg_join[b], cudaEventDisableTiming));
@@ -154,6 +159,198 @@ int seg_launch_groups(hpcs_ctx* ctx, const SegDesc* d_desc, const std::vector<Se
                                                : launch_groups_mode<RANK_PEER_MASK>(ctx, d_desc, groups, d_queues, s);
 }
 
+// ---- grid-level path (seg_grid.cuh) -------------------------------------------------------
+namespace {
+int dtype_bytes(int dtype) { return dtype >= HPCS_U64 ? 8 : 4; }
+
+template <class U, int MODE>
+void grid_geometry(int64_t n, ChunkGeometry& g) {
+  using S = ChunkShape<U, NoValue, MODE>;
+  const int64_t tiles = (n + S::TILE - 1) / S::TILE;
+  int64_t want = (tiles + SEG_GRID_TILES_PER_RANGE - 1) / SEG_GRID_TILES_PER_RANGE;
+  if (want > S::MAX_RANGES) want = S::MAX_RANGES;
+  if (want < 1) want = 1;
+  g = chunk_geometry(n, S::TILE, int(want));
+}
+
+template <class U, int KIND, int MODE>
+int grid_launch_set(hpcs_ctx* ctx, const SegGridSet& set, const SortArgs* d_args, const int2* d_map,
+                    cudaStream_t s) {
+  using C = ChunkConfig<U, NoValue, MODE>;
+  using L = ChunkSmem<U, NoValue, C::NT, C::KPT, MODE>;
+  constexpr int P = int(sizeof(U));
+  const SortArgs* a = d_args + set.first;
+  const int2* m = d_map + set.map_first;
+  seg_hist_all_digits_kernel<U, KIND, HIST_NT><<<set.ctas, HIST_NT, HistSmem<U>::BYTES, s>>>(a, m);
+  HPCS_CUDA(cudaGetLastError());
+  for (int p = 0; p < P; p++) {
+    seg_chunk_pass_kernel<U, KIND, NoValue, C::NT, C::KPT, MODE><<<set.ctas, C::NT, L::bytes(set.max_ranges), s>>>(a, m, p);
+    HPCS_CUDA(cudaGetLastError());
+  }
+  seg_finalize_kernel<U><<<set.ctas, 256, 0, s>>>(a, m, device_error_word(ctx));
+  HPCS_CUDA(cudaGetLastError());
+  return HPCS_OK;
+}
+
+template <class U, int KIND, int MODE>
+int grid_setup_type(hpcs_ctx* ctx) {
+  using C = ChunkConfig<U, NoValue, MODE>;
+  static int done[64] = {0};
+  if (done[ctx->device & 63]) return HPCS_OK;
+  HPCS_CUDA(cudaFuncSetAttribute(seg_hist_all_digits_kernel<U, KIND, HIST_NT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(HistSmem<U>::BYTES)));
+  HPCS_CUDA(cudaFuncSetAttribute(seg_chunk_pass_kernel<U, KIND, NoValue, C::NT, C::KPT, MODE>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(MAX_DYN_SMEM)));
+  done[ctx->device & 63] = 1;
+  return HPCS_OK;
+}
+
+template <int MODE>
+int grid_dispatch(hpcs_ctx* ctx, const SegGridSet* set, const SortArgs* d_args, const int2* d_map, cudaStream_t s) {
+  const bool setup = set == nullptr;
+  for (int dt = HPCS_U32; dt <= HPCS_F64; dt++) {
+    if (!setup && set->dtype != dt) continue;
+    int rc = HPCS_OK;
+    switch (dt) {
+      case HPCS_U32: rc = setup ? grid_setup_type<uint32_t, KIND_UNSIGNED, MODE>(ctx) : grid_launch_set<uint32_t, KIND_UNSIGNED, MODE>(ctx, *set, d_args, d_map, s); break;
+      case HPCS_I32: rc = setup ? grid_setup_type<uint32_t, KIND_SIGNED, MODE>(ctx) : grid_launch_set<uint32_t, KIND_SIGNED, MODE>(ctx, *set, d_args, d_map, s); break;
+      case HPCS_F32: rc = setup ? grid_setup_type<uint32_t, KIND_FLOAT, MODE>(ctx) : grid_launch_set<uint32_t, KIND_FLOAT, MODE>(ctx, *set, d_args, d_map, s); break;
+      case HPCS_U64: rc = setup ? grid_setup_type<uint64_t, KIND_UNSIGNED, MODE>(ctx) : grid_launch_set<uint64_t, KIND_UNSIGNED, MODE>(ctx, *set, d_args, d_map, s); break;
+      case HPCS_I64: rc = setup ? grid_setup_type<uint64_t, KIND_SIGNED, MODE>(ctx) : grid_launch_set<uint64_t, KIND_SIGNED, MODE>(ctx, *set, d_args, d_map, s); break;
+      default: rc = setup ? grid_setup_type<uint64_t, KIND_FLOAT, MODE>(ctx) : grid_launch_set<uint64_t, KIND_FLOAT, MODE>(ctx, *set, d_args, d_map, s); break;
+    }
+    if (rc != HPCS_OK) return rc;
+  }
+  return HPCS_OK;
+}
+}  // namespace
+
+int seg_grid_build(const hpcs_segment* segs, const std::vector<int64_t>& idx, int mode, int skip_trivial,
+                   uint64_t spin_limit_ns, SegGrid& grid) {
+  grid = SegGrid();
+  grid.mode = mode;
+  auto align = [](size_t x) { return (x + 255) / 256 * 256; };
+  for (int dt = HPCS_U32; dt <= HPCS_F64; dt++) {
+    std::vector<int64_t> mine;
+    for (int64_t i : idx)
+      if (segs[i].dtype == dt) mine.push_back(i);
+    if (mine.empty()) continue;
+    SegGridSet set;
+    set.dtype = dt;
+    set.first = int(grid.args.size());
+    set.count = int(mine.size());
+    set.map_first = int(grid.map.size());
+    set.plan_off = grid.scratch;
+    set.plan_bytes = align(mine.size() * sizeof(SortPlan));
+    grid.scratch += set.plan_bytes;
+    const int w = dtype_bytes(dt);
+    const int P = w;
+    for (size_t q = 0; q < mine.size(); q++) {
+      const hpcs_segment& sg = segs[mine[q]];
+      ChunkGeometry g;
+      if (w == 4) {
+        if (mode == RANK_ORDERED_ATOMIC) grid_geometry<uint32_t, RANK_ORDERED_ATOMIC>(sg.n, g);
+        else grid_geometry<uint32_t, RANK_PEER_MASK>(sg.n, g);
+      } else {
+        if (mode == RANK_ORDERED_ATOMIC) grid_geometry<uint64_t, RANK_ORDERED_ATOMIC>(sg.n, g);
+        else grid_geometry<uint64_t, RANK_PEER_MASK>(sg.n, g);
+      }
+      SortArgs a{};
+      a.keys_a = sg.keys;
+      a.n = sg.n;
+      // scratch offsets (+1, so 0 stays "none") until relocation
+      a.keys_b = reinterpret_cast<void*>(grid.scratch + 1);
+      grid.scratch += align(size_t(sg.n) * w);
+      a.chunk_hist = reinterpret_cast<uint32_t*>(grid.scratch + 1);
+      grid.scratch += align(size_t(g.chunks) * (P + 3) * RADIX * 4);
+      a.plan = reinterpret_cast<SortPlan*>(set.plan_off + q * sizeof(SortPlan) + 1);
+      a.chunks = g.chunks;
+      a.chunk_keys = g.chunk_keys;
+      a.chunk_magic = g.magic;
+      a.skip_trivial = skip_trivial;
+      a.poison_tile = -1;
+      a.spin_limit_ns = spin_limit_ns;
+      a.trace_pass = -1;
+      grid.args.push_back(a);
+      for (int r = 0; r < g.chunks; r++) grid.map.push_back(make_int2(int(q), r));
+      if (g.chunks > set.max_ranges) set.max_ranges = g.chunks;
+    }
+    set.ctas = int(grid.map.size()) - set.map_first;
+    grid.sets.push_back(set);
+  }
+  return HPCS_OK;
+}
+
+void seg_grid_relocate(SegGrid& grid, void* base) {
+  unsigned char* b = static_cast<unsigned char*>(base);
+  auto fix = [&](auto* p) { return reinterpret_cast<decltype(p)>(b + (reinterpret_cast<size_t>(p) - 1)); };
+  for (auto& a : grid.args) {
+    a.keys_b = fix(static_cast<unsigned char*>(a.keys_b));
+    a.chunk_hist = fix(a.chunk_hist);
+    a.plan = fix(a.plan);
+  }
+  // the next-digit tables follow each array's per-range counts
+  for (const auto& set : grid.sets) {
+    const int P = dtype_bytes(set.dtype);
+    for (int q = 0; q < set.count; q++) {
+      SortArgs& a = grid.args[size_t(set.first + q)];
+      a.ctab = a.chunk_hist + size_t(a.chunks) * P * RADIX;
+    }
+  }
+}
+
+int seg_grid_setup(hpcs_ctx* ctx, const SegGrid& grid) {
+  if (grid.sets.empty()) return HPCS_OK;
+  return grid.mode == RANK_ORDERED_ATOMIC ? grid_dispatch<RANK_ORDERED_ATOMIC>(ctx, nullptr, nullptr, nullptr, nullptr)
+                                          : grid_dispatch<RANK_PEER_MASK>(ctx, nullptr, nullptr, nullptr, nullptr);
+}
+
+int seg_grid_launch(hpcs_ctx* ctx, const SegGrid& grid, const SortArgs* d_args, const int2* d_map, cudaStream_t s) {
+  for (const auto& set : grid.sets) {
+    const SortPlan* plan0 = grid.args[size_t(set.first)].plan;
+    HPCS_CUDA(cudaMemsetAsync(const_cast<SortPlan*>(plan0), 0, set.plan_bytes, s));
+    const int rc = grid.mode == RANK_ORDERED_ATOMIC ? grid_dispatch<RANK_ORDERED_ATOMIC>(ctx, &set, d_args, d_map, s)
+                                                    : grid_dispatch<RANK_PEER_MASK>(ctx, &set, d_args, d_map, s);
+    if (rc != HPCS_OK) return rc;
+  }
+  return HPCS_OK;
+}
+
+namespace {
+// Splits a batch into the grid-level arrays (their indices) and the others (copied out).
+void seg_split(const hpcs_segment* segs, int64_t nsegs, std::vector<hpcs_segment>& rest,
+               std::vector<int64_t>& grid_idx) {
+  rest.clear();
+  grid_idx.clear();
+  for (int64_t i = 0; i < nsegs; i++) {
+    if (seg_grid_eligible(segs[i])) grid_idx.push_back(i);
+    else rest.push_back(segs[i]);
+  }
+}
+
+// The whole batch on stream s: the grid-level sets on their own branch, the other arrays' groups
+// as before (the heaviest on s, the others on the helper streams).
+int seg_launch_all(hpcs_ctx* ctx, const SegDesc* d_desc, const std::vector<SegGroup>& groups, uint32_t* d_queues,
+                   const SegGrid& grid, const SortArgs* d_args, const int2* d_map, cudaStream_t s) {
+  int rc;
+  const bool branch = !grid.sets.empty();
+  if (branch) {
+    if ((rc = ensure_seg_streams(ctx)) != HPCS_OK) return rc;
+    HPCS_CUDA(cudaEventRecord(ctx->seg_grid_fork, s));
+    HPCS_CUDA(cudaStreamWaitEvent(ctx->seg_grid_stream, ctx->seg_grid_fork, 0));
+    if ((rc = seg_grid_launch(ctx, grid, d_args, d_map, ctx->seg_grid_stream)) != HPCS_OK) return rc;
+  }
+  if ((rc = seg_launch_groups(ctx, d_desc, groups, d_queues, s)) != HPCS_OK) return rc;
+  if (branch) {
+    HPCS_CUDA(cudaEventRecord(ctx->seg_grid_join, ctx->seg_grid_stream));
+    HPCS_CUDA(cudaStreamWaitEvent(s, ctx->seg_grid_join, 0));
+  }
+  return HPCS_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+}  // namespace
+
 }  // namespace hpcs
 
 using namespace hpcs;
@@ -162,35 +359,65 @@ extern "C" {
 
 int hpcs_sort_segmented_dev(hpcs_ctx* ctx, const hpcs_segment* segs, int64_t nsegs, void* stream) {
   if (!ctx) return fail(HPCS_ERR_NULL, "ctx is NULL");
+  int rc = validate(segs, nsegs);
+  if (rc != HPCS_OK || nsegs == 0) return rc;
+  std::vector<hpcs_segment> rest;
+  std::vector<int64_t> grid_idx;
+  seg_split(segs, nsegs, rest, grid_idx);
   std::vector<SegDesc> table;
   std::vector<SegGroup> groups;
   size_t scratch = 0;
-  int rc = seg_build_groups(ctx->seg_tuning, segs, nsegs, table, groups, scratch);
-  if (rc != HPCS_OK || nsegs == 0) return rc;
+  if ((rc = seg_build_groups(ctx->seg_tuning, rest.data(), int64_t(rest.size()), table, groups, scratch)) != HPCS_OK)
+    return rc;
+  SegGrid grid;
+  if ((rc = seg_grid_build(segs, grid_idx, ctx->rank_mode, ctx->cfg.skip_trivial_passes,
+                           uint64_t(ctx->cfg.spin_limit_ns), grid)) != HPCS_OK)
+    return rc;
   DeviceGuard2 g(ctx->device);
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
   if ((rc = enter_stream(ctx, s)) != HPCS_OK) return rc;
+  if ((rc = seg_grid_setup(ctx, grid)) != HPCS_OK) return rc;
+  const size_t block_scratch = align256(scratch);
   const size_t desc_bytes = table.size() * sizeof(SegDesc);
-  if ((rc = ensure(ctx, ctx->aux0, scratch ? scratch : 256)) != HPCS_OK) return rc;
+  const size_t args_bytes = align256(grid.args.size() * sizeof(SortArgs));
+  const size_t map_bytes = grid.map.size() * sizeof(int2);
+  if ((rc = ensure(ctx, ctx->aux0, block_scratch + grid.scratch + 256)) != HPCS_OK) return rc;
   if ((rc = ensure(ctx, ctx->aux1, desc_bytes + 256 + groups.size() * 4)) != HPCS_OK) return rc;
+  if ((rc = ensure(ctx, ctx->aux2, args_bytes + map_bytes + 256)) != HPCS_OK) return rc;
   seg_relocate(table, groups, ctx->aux0.ptr);
+  seg_grid_relocate(grid, static_cast<unsigned char*>(ctx->aux0.ptr) + block_scratch);
   SegDesc* d_desc = static_cast<SegDesc*>(ctx->aux1.ptr);
   uint32_t* d_queues = reinterpret_cast<uint32_t*>(static_cast<unsigned char*>(ctx->aux1.ptr) + (desc_bytes + 255) / 256 * 256);
-  // the host table must outlive the copy: copy synchronously with respect to this stream
-  HPCS_CUDA(cudaMemcpyAsync(d_desc, table.data(), desc_bytes, cudaMemcpyHostToDevice, s));
+  SortArgs* d_args = static_cast<SortArgs*>(ctx->aux2.ptr);
+  int2* d_map = reinterpret_cast<int2*>(static_cast<unsigned char*>(ctx->aux2.ptr) + args_bytes);
+  // the host tables must outlive the copies: copy synchronously with respect to this stream
+  if (desc_bytes) HPCS_CUDA(cudaMemcpyAsync(d_desc, table.data(), desc_bytes, cudaMemcpyHostToDevice, s));
+  if (!grid.args.empty()) {
+    HPCS_CUDA(cudaMemcpyAsync(d_args, grid.args.data(), grid.args.size() * sizeof(SortArgs), cudaMemcpyHostToDevice, s));
+    HPCS_CUDA(cudaMemcpyAsync(d_map, grid.map.data(), map_bytes, cudaMemcpyHostToDevice, s));
+  }
   HPCS_CUDA(cudaStreamSynchronize(s));
   KernelTimer kt(ctx, s, HPCS_K_SEGMENTED);
-  return seg_launch_groups(ctx, d_desc, groups, d_queues, s);
+  return seg_launch_all(ctx, d_desc, groups, d_queues, grid, d_args, d_map, s);
 }
 
 int hpcs_segplan_create(hpcs_ctx* ctx, const hpcs_segment* segs, int64_t nsegs, hpcs_segplan** out) {
   if (!ctx || !out) return fail(HPCS_ERR_NULL, "ctx or out is NULL");
   *out = nullptr;
+  int rc = validate(segs, nsegs);
+  if (rc != HPCS_OK) return rc;
+  std::vector<hpcs_segment> rest;
+  std::vector<int64_t> grid_idx;
+  seg_split(segs, nsegs, rest, grid_idx);
   std::vector<SegDesc> table;
   std::vector<SegGroup> groups;
   size_t scratch = 0;
-  int rc = seg_build_groups(ctx->seg_tuning, segs, nsegs, table, groups, scratch);
-  if (rc != HPCS_OK) return rc;
+  if ((rc = seg_build_groups(ctx->seg_tuning, rest.data(), int64_t(rest.size()), table, groups, scratch)) != HPCS_OK)
+    return rc;
+  SegGrid grid;
+  if ((rc = seg_grid_build(segs, grid_idx, ctx->rank_mode, ctx->cfg.skip_trivial_passes,
+                           uint64_t(ctx->cfg.spin_limit_ns), grid)) != HPCS_OK)
+    return rc;
   DeviceGuard2 g(ctx->device);
   auto* p = new hpcs_segplan();
   p->ctx = ctx;
@@ -201,13 +428,30 @@ int hpcs_segplan_create(hpcs_ctx* ctx, const hpcs_segment* segs, int64_t nsegs, 
   };
   const size_t desc_bytes = table.size() * sizeof(SegDesc);
   const size_t queue_off = (desc_bytes + 255) / 256 * 256;
+  const size_t block_scratch = align256(scratch);
+  const size_t args_bytes = align256(grid.args.size() * sizeof(SortArgs));
+  const size_t map_bytes = grid.map.size() * sizeof(int2);
   cudaError_t e;
   if ((e = cudaMalloc(&p->d_desc, queue_off + 256 + groups.size() * 4)) != cudaSuccess)
     return cleanup(cuda_fail(e, "cudaMalloc"));
   p->d_queue = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(p->d_desc) + queue_off);
-  if (scratch && (e = cudaMalloc(&p->d_scratch, scratch)) != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc"));
-  p->scratch_bytes = scratch;
+  const size_t all_scratch = block_scratch + grid.scratch;
+  if (all_scratch && (e = cudaMalloc(&p->d_scratch, all_scratch)) != cudaSuccess)
+    return cleanup(cuda_fail(e, "cudaMalloc"));
+  p->scratch_bytes = all_scratch;
   seg_relocate(table, groups, p->d_scratch);
+  SortArgs* d_args = nullptr;
+  int2* d_map = nullptr;
+  if (!grid.sets.empty()) {
+    seg_grid_relocate(grid, static_cast<unsigned char*>(p->d_scratch) + block_scratch);
+    if ((e = cudaMalloc(&p->d_grid, args_bytes + map_bytes)) != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc"));
+    d_args = static_cast<SortArgs*>(p->d_grid);
+    d_map = reinterpret_cast<int2*>(static_cast<unsigned char*>(p->d_grid) + args_bytes);
+    if ((e = cudaMemcpy(d_args, grid.args.data(), grid.args.size() * sizeof(SortArgs), cudaMemcpyHostToDevice)) !=
+            cudaSuccess ||
+        (e = cudaMemcpy(d_map, grid.map.data(), map_bytes, cudaMemcpyHostToDevice)) != cudaSuccess)
+      return cleanup(cuda_fail(e, "cudaMemcpy"));
+  }
   if (desc_bytes && (e = cudaMemcpy(p->d_desc, table.data(), desc_bytes, cudaMemcpyHostToDevice)) != cudaSuccess)
     return cleanup(cuda_fail(e, "cudaMemcpy"));
   if ((e = cudaStreamCreateWithFlags(&p->capture_stream, cudaStreamNonBlocking)) != cudaSuccess)
@@ -218,6 +462,8 @@ int hpcs_segplan_create(hpcs_ctx* ctx, const hpcs_segment* segs, int64_t nsegs, 
     std::vector<SegGroup> warm = groups;
     for (auto& wg : warm) wg.count = 0;
     if ((rc = seg_launch_groups(ctx, p->d_desc, warm, p->d_queue, p->capture_stream)) != HPCS_OK) return cleanup(rc);
+    if ((rc = seg_grid_setup(ctx, grid)) != HPCS_OK) return cleanup(rc);
+    if (!grid.sets.empty() && (rc = ensure_seg_streams(ctx)) != HPCS_OK) return cleanup(rc);
     if ((e = cudaStreamSynchronize(p->capture_stream)) != cudaSuccess) return cleanup(cuda_fail(e, "sync"));
   }
   const bool was_profiling = ctx->profile;
@@ -226,7 +472,7 @@ int hpcs_segplan_create(hpcs_ctx* ctx, const hpcs_segment* segs, int64_t nsegs, 
     ctx->profile = was_profiling;
     return cleanup(cuda_fail(e, "cudaStreamBeginCapture"));
   }
-  rc = seg_launch_groups(ctx, p->d_desc, groups, p->d_queue, p->capture_stream);
+  rc = seg_launch_all(ctx, p->d_desc, groups, p->d_queue, grid, d_args, d_map, p->capture_stream);
   e = cudaStreamEndCapture(p->capture_stream, &p->graph);
   ctx->profile = was_profiling;
   if (rc != HPCS_OK) return cleanup(rc);
@@ -257,6 +503,7 @@ int hpcs_segplan_destroy(hpcs_segplan* p) {
   if (p->graph) cudaGraphDestroy(p->graph);
   if (p->capture_stream) cudaStreamDestroy(p->capture_stream);
   if (p->d_scratch) cudaFree(p->d_scratch);
+  if (p->d_grid) cudaFree(p->d_grid);
   if (p->d_desc) cudaFree(p->d_desc);
   delete p;
   return HPCS_OK;

@@ -74,6 +74,9 @@ struct hpcs_ctx {
   cudaStream_t seg_streams[SEG_BRANCHES] = {};
   cudaEvent_t seg_fork = nullptr;
   cudaEvent_t seg_join[SEG_BRANCHES] = {};
+  // the grid-level path of the batched sort runs on its own branch
+  cudaStream_t seg_grid_stream = nullptr;
+  cudaEvent_t seg_grid_fork = nullptr, seg_grid_join = nullptr;
 };
 
 namespace hpcs {

@@ -184,3 +184,47 @@ def test_builtin_table_is_the_tuned_record(ctx):
 
     rec = json.load(open(os.path.join(os.path.dirname(autotune.__file__), "tune", "b200_148sm.json")))
     assert ctx.seg_tuning == rec["table"]
+
+
+GRID_LENGTHS = [262_144, 262_145, 16_384 * 8 * 3 - 1, 1_048_576 + 7, 2_500_001]
+
+
+@pytest.mark.parametrize("use_plan", [False, True], ids=["one_shot", "plan_twice"])
+def test_grid_level_arrays(ctx, orc, use_plan):
+    """Arrays of at least 2^18 aligned keys go to the grid-level path (many CTAs per array, the
+    plain sort's kernels per range); unaligned ones of the same length stay on the block-level
+    path.  Constant and low-byte-only arrays make passes the identity (an odd number runs: the
+    copy back).  Every array must equal the oracle's sort of it alone."""
+    import torch
+
+    host = []
+    for i, n in enumerate(GRID_LENGTHS):
+        for j, dt in enumerate(DT):
+            a = datagen.by_name(dt, n, seed=40 + 10 * i + j)
+            if (i + j) % 5 == 3:
+                a = a.copy()
+                a.view(np.uint32 if a.dtype.itemsize == 4 else np.uint64)[:] &= 0xFF  # low byte only
+            if (i + j) % 7 == 5:
+                a = np.full_like(a, a[0])  # every pass the identity
+            host.append((a, dt))
+    offsets = [1 if k % 4 == 1 else 0 for k in range(len(host))]  # every fourth array unaligned
+    devs = [to_dev(a, offset_elems=o) for (a, _), o in zip(host, offsets)]
+    segs = [(t, d) for t, (_, d) in zip(devs, host)]
+    if use_plan:
+        plan = ctx.segplan(segs)
+        try:
+            for rep in range(2):
+                if rep:  # restore the inputs: the second replay sorts them again
+                    for t, (a, _), o in zip(devs, host, offsets):
+                        t.copy_(to_dev(a))
+                plan.execute(stream=native.torch_stream())
+                torch.cuda.synchronize()
+                ctx.synchronize()
+                check(host, devs, orc)
+        finally:
+            plan.close()
+    else:
+        ctx.sort_segmented_dev(segs, stream=native.torch_stream())
+        torch.cuda.synchronize()
+        ctx.synchronize()
+        check(host, devs, orc)
