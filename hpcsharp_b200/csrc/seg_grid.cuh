@@ -1,8 +1,9 @@
 // Grid-level path of the batched segmented sort: the longest arrays of a batch are spread over
 // many CTAs each.
 //
-// An array of at least SEG_GRID_MIN_KEYS keys (16-byte aligned) is cut into key ranges of at most
-// SEG_GRID_TILES_PER_RANGE tiles of the plain sort's chunked pass, and every range becomes one
+// An array of at least SEG_GRID_MIN_KEYS keys (16-byte aligned; both numbers are context settings)
+// is cut into key ranges of at most SEG_GRID_TILES_PER_RANGE tiles of the plain sort's chunked
+// pass, and every range becomes one
 // CTA of the plain sort's own kernels: the fused histogram (which also builds the array's plan in
 // its last CTA), one chunked digit pass per digit, and a copy back when an odd number of passes
 // ran.  The arrays of one key type share each launch: CTA c reads (array, range) from a map and the
@@ -18,8 +19,11 @@
 
 namespace hpcs {
 
-constexpr int64_t SEG_GRID_MIN_KEYS = int64_t(1) << 18;
-constexpr int SEG_GRID_TILES_PER_RANGE = 8;
+// Defaults, from a sweep on B200 over 65,536 arrays of log-uniform length on [32, 2^20] (4- and
+// 8-byte keys): thresholds 8 Ki-256 Ki and 8-64 tiles per CTA were within 2% of each other
+// from 32 Ki to 128 Ki keys and 32 tiles, and one CTA per array (no grid level) was 14% slower.
+constexpr int64_t SEG_GRID_MIN_KEYS = int64_t(1) << 16;
+constexpr int SEG_GRID_TILES_PER_RANGE = 32;
 
 // The grid-level arrays of one key type: args[first, first + count) and map[map_first,
 // map_first + ctas) (map entries index args relative to `first`).
@@ -40,13 +44,22 @@ struct SegGrid {
   int mode = RANK_ORDERED_ATOMIC;
 };
 
-inline bool seg_grid_eligible(const hpcs_segment& sg) {
-  return sg.n >= SEG_GRID_MIN_KEYS && (reinterpret_cast<uintptr_t>(sg.keys) & 15) == 0;
+// The context's length threshold (hpcs_config.seg_grid_min_keys; <0: none) and tiles per CTA.
+inline int64_t seg_grid_min_keys(const hpcs_config& cfg) {
+  return cfg.seg_grid_min_keys < 0 ? INT64_MAX : cfg.seg_grid_min_keys == 0 ? SEG_GRID_MIN_KEYS : cfg.seg_grid_min_keys;
+}
+inline int seg_grid_tiles(const hpcs_config& cfg) {
+  return cfg.seg_grid_tiles > 0 ? cfg.seg_grid_tiles : SEG_GRID_TILES_PER_RANGE;
 }
 
-// Builds the grid-level sets of the arrays `idx` (all eligible) for ranking mode `mode`.
+inline bool seg_grid_eligible(const hpcs_segment& sg, int64_t min_keys) {
+  return sg.n >= min_keys && (reinterpret_cast<uintptr_t>(sg.keys) & 15) == 0;
+}
+
+// Builds the grid-level sets of the arrays `idx` (all eligible) for ranking mode `mode`, with
+// ranges of at most `tiles_per_range` tiles.
 int seg_grid_build(const hpcs_segment* segs, const std::vector<int64_t>& idx, int mode, int skip_trivial,
-                   uint64_t spin_limit_ns, SegGrid& grid);
+                   uint64_t spin_limit_ns, int tiles_per_range, SegGrid& grid);
 // Turns the scratch offsets into device pointers.
 void seg_grid_relocate(SegGrid& grid, void* base);
 // Sets the kernels' shared-memory attributes (outside any stream capture).

@@ -164,10 +164,10 @@ namespace {
 int dtype_bytes(int dtype) { return dtype >= HPCS_U64 ? 8 : 4; }
 
 template <class U, int MODE>
-void grid_geometry(int64_t n, ChunkGeometry& g) {
+void grid_geometry(int64_t n, int tiles_per_range, ChunkGeometry& g) {
   using S = ChunkShape<U, NoValue, MODE>;
   const int64_t tiles = (n + S::TILE - 1) / S::TILE;
-  int64_t want = (tiles + SEG_GRID_TILES_PER_RANGE - 1) / SEG_GRID_TILES_PER_RANGE;
+  int64_t want = (tiles + tiles_per_range - 1) / tiles_per_range;
   if (want > S::MAX_RANGES) want = S::MAX_RANGES;
   if (want < 1) want = 1;
   g = chunk_geometry(n, S::TILE, int(want));
@@ -226,7 +226,7 @@ int grid_dispatch(hpcs_ctx* ctx, const SegGridSet* set, const SortArgs* d_args, 
 }  // namespace
 
 int seg_grid_build(const hpcs_segment* segs, const std::vector<int64_t>& idx, int mode, int skip_trivial,
-                   uint64_t spin_limit_ns, SegGrid& grid) {
+                   uint64_t spin_limit_ns, int tiles_per_range, SegGrid& grid) {
   grid = SegGrid();
   grid.mode = mode;
   auto align = [](size_t x) { return (x + 255) / 256 * 256; };
@@ -249,11 +249,11 @@ int seg_grid_build(const hpcs_segment* segs, const std::vector<int64_t>& idx, in
       const hpcs_segment& sg = segs[mine[q]];
       ChunkGeometry g;
       if (w == 4) {
-        if (mode == RANK_ORDERED_ATOMIC) grid_geometry<uint32_t, RANK_ORDERED_ATOMIC>(sg.n, g);
-        else grid_geometry<uint32_t, RANK_PEER_MASK>(sg.n, g);
+        if (mode == RANK_ORDERED_ATOMIC) grid_geometry<uint32_t, RANK_ORDERED_ATOMIC>(sg.n, tiles_per_range, g);
+        else grid_geometry<uint32_t, RANK_PEER_MASK>(sg.n, tiles_per_range, g);
       } else {
-        if (mode == RANK_ORDERED_ATOMIC) grid_geometry<uint64_t, RANK_ORDERED_ATOMIC>(sg.n, g);
-        else grid_geometry<uint64_t, RANK_PEER_MASK>(sg.n, g);
+        if (mode == RANK_ORDERED_ATOMIC) grid_geometry<uint64_t, RANK_ORDERED_ATOMIC>(sg.n, tiles_per_range, g);
+        else grid_geometry<uint64_t, RANK_PEER_MASK>(sg.n, tiles_per_range, g);
       }
       SortArgs a{};
       a.keys_a = sg.keys;
@@ -318,12 +318,12 @@ int seg_grid_launch(hpcs_ctx* ctx, const SegGrid& grid, const SortArgs* d_args, 
 
 namespace {
 // Splits a batch into the grid-level arrays (their indices) and the others (copied out).
-void seg_split(const hpcs_segment* segs, int64_t nsegs, std::vector<hpcs_segment>& rest,
+void seg_split(const hpcs_segment* segs, int64_t nsegs, int64_t min_keys, std::vector<hpcs_segment>& rest,
                std::vector<int64_t>& grid_idx) {
   rest.clear();
   grid_idx.clear();
   for (int64_t i = 0; i < nsegs; i++) {
-    if (seg_grid_eligible(segs[i])) grid_idx.push_back(i);
+    if (seg_grid_eligible(segs[i], min_keys)) grid_idx.push_back(i);
     else rest.push_back(segs[i]);
   }
 }
@@ -363,7 +363,7 @@ int hpcs_sort_segmented_dev(hpcs_ctx* ctx, const hpcs_segment* segs, int64_t nse
   if (rc != HPCS_OK || nsegs == 0) return rc;
   std::vector<hpcs_segment> rest;
   std::vector<int64_t> grid_idx;
-  seg_split(segs, nsegs, rest, grid_idx);
+  seg_split(segs, nsegs, seg_grid_min_keys(ctx->cfg), rest, grid_idx);
   std::vector<SegDesc> table;
   std::vector<SegGroup> groups;
   size_t scratch = 0;
@@ -371,7 +371,7 @@ int hpcs_sort_segmented_dev(hpcs_ctx* ctx, const hpcs_segment* segs, int64_t nse
     return rc;
   SegGrid grid;
   if ((rc = seg_grid_build(segs, grid_idx, ctx->rank_mode, ctx->cfg.skip_trivial_passes,
-                           uint64_t(ctx->cfg.spin_limit_ns), grid)) != HPCS_OK)
+                           uint64_t(ctx->cfg.spin_limit_ns), seg_grid_tiles(ctx->cfg), grid)) != HPCS_OK)
     return rc;
   DeviceGuard2 g(ctx->device);
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
@@ -408,7 +408,7 @@ int hpcs_segplan_create(hpcs_ctx* ctx, const hpcs_segment* segs, int64_t nsegs, 
   if (rc != HPCS_OK) return rc;
   std::vector<hpcs_segment> rest;
   std::vector<int64_t> grid_idx;
-  seg_split(segs, nsegs, rest, grid_idx);
+  seg_split(segs, nsegs, seg_grid_min_keys(ctx->cfg), rest, grid_idx);
   std::vector<SegDesc> table;
   std::vector<SegGroup> groups;
   size_t scratch = 0;
@@ -416,7 +416,7 @@ int hpcs_segplan_create(hpcs_ctx* ctx, const hpcs_segment* segs, int64_t nsegs, 
     return rc;
   SegGrid grid;
   if ((rc = seg_grid_build(segs, grid_idx, ctx->rank_mode, ctx->cfg.skip_trivial_passes,
-                           uint64_t(ctx->cfg.spin_limit_ns), grid)) != HPCS_OK)
+                           uint64_t(ctx->cfg.spin_limit_ns), seg_grid_tiles(ctx->cfg), grid)) != HPCS_OK)
     return rc;
   DeviceGuard2 g(ctx->device);
   auto* p = new hpcs_segplan();

@@ -223,36 +223,54 @@ __global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) select_compact_kernel
 }
 
 // ---- top-k with one read of the keys ---------------------------------------------------
-// A strided sample of the keys gives a threshold T that about m = TOPK_MARGIN(k) sampled keys
-// reach; one read of all keys then keeps the keys at or above T (the candidates).  When at
+// A strided sample of the keys gives a threshold T that about m sampled keys reach; one read of all keys then keeps the keys at or above T (the candidates).  When at
 // least k keys were kept, every one of the k largest is among them and the radix select runs
 // over the candidates only; otherwise (a sample far off, or tiny inputs) the select falls back
 // to the two reads of the full path.  The choice is made on the device (SelectState::mode):
 // the kernels of the path not taken return at their first instruction.
-constexpr int TOPK_SAMPLE = 8192;
+template <class U>
+__host__ __device__ constexpr int topk_sample_size() {
+  return sizeof(U) == 4 ? 32768 : 16384;  // 32 / 16 keys per thread in registers
+}
 constexpr int TOPK_SAMPLE_NT = 1024;
 
-// One CTA: the ordered sample value of rank (S - m), S = TOPK_SAMPLE samples at stride n / S,
-// by an MSD radix select in shared memory.  Writes st->threshold (0 = keep every key).
+// One CTA: the SelectState set up for the k largest of n keys (rank n - k), and the ordered
+// sample value of rank (S - m) among S = topk_sample_size<U>() keys at stride n / S, by an MSD
+// radix select in shared memory (per level a histogram of the samples matching the prefix and
+// a scan of its 256 bins by 8 warps).  Writes st->threshold (0 = keep every key).
 template <class U, int KIND>
 __global__ void __launch_bounds__(TOPK_SAMPLE_NT) topk_sample_kernel(const U* __restrict__ keys, int64_t n,
-                                                                     int64_t m, SelectState* st) {
+                                                                     int64_t k, int64_t m, SelectState* st) {
   using KO = KeyOrder<U, KIND>;
   constexpr int BITS = int(sizeof(U) * 8);
-  constexpr int PER = TOPK_SAMPLE / TOPK_SAMPLE_NT;
+  constexpr int S = topk_sample_size<U>();
+  constexpr int PER = S / TOPK_SAMPLE_NT;
   __shared__ uint32_t hist[256];
+  __shared__ uint32_t s_wsum[8];
   __shared__ uint32_t s_bin, s_below;
-  const int tid = threadIdx.x;
-  if (n < int64_t(4) * TOPK_SAMPLE || m >= TOPK_SAMPLE) {  // too few keys to sample: keep them all
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    st->n_total = n;
+    st->prefix = 0;
+    st->mask = 0;
+    st->rank = n - k;
+    st->less = 0;
+    st->eq = 0;
+    st->cand_count = 0;
+    st->gathered = 0;
+    st->mode = SEL_MODE_FULL;
+  }
+  if (tid < 256) st->hist[tid] = 0;
+  if (n < int64_t(4) * S || m >= S) {  // too few keys to sample: keep them all
     if (tid == 0) st->threshold = 0;
     return;
   }
-  const int64_t stride = n / TOPK_SAMPLE;
+  const int64_t stride = n / S;
   U o[PER];
 #pragma unroll
   for (int q = 0; q < PER; q++) o[q] = KO::to_ordered(keys[int64_t(tid + q * TOPK_SAMPLE_NT) * stride]);
   // rank (0-based, ascending) of the threshold among the samples
-  uint32_t rank = uint32_t(TOPK_SAMPLE - m);
+  uint32_t rank = uint32_t(S - m);
   U prefix = 0, mask = 0;
   for (int shift = BITS - 8; shift >= 0; shift -= 8) {
     if (tid < 256) hist[tid] = 0;
@@ -261,18 +279,27 @@ __global__ void __launch_bounds__(TOPK_SAMPLE_NT) topk_sample_kernel(const U* __
     for (int q = 0; q < PER; q++)
       if ((o[q] & mask) == prefix) atomicAdd(&hist[uint32_t(o[q] >> shift) & 0xFFu], 1u);
     __syncthreads();
-    if (tid == 0) {  // 256 bins: a serial scan is a few hundred cycles per level
-      uint32_t below = 0;
-      int bin = 255;
-      for (int b = 0; b < 256; b++) {
-        if (rank < below + hist[b]) {
-          bin = b;
-          break;
-        }
-        below += hist[b];
+    uint32_t c = 0, incl = 0;
+    if (tid < 256) {
+      c = hist[tid];
+      incl = c;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+        if (lane >= off) incl += y;
       }
-      s_bin = uint32_t(bin);
-      s_below = below;
+      if (lane == 31) s_wsum[warp] = incl;
+    }
+    __syncthreads();
+    if (tid < 256) {
+      uint32_t base = 0;
+      for (int w = 0; w < warp; w++) base += s_wsum[w];
+      const uint32_t excl = base + incl - c;
+      // the bins' ranges [excl, excl + c) are disjoint: exactly one thread matches
+      if ((c > 0u && rank >= excl && rank < excl + c) || (tid == 255 && rank >= excl + c)) {
+        s_bin = uint32_t(tid);
+        s_below = excl;
+      }
     }
     __syncthreads();
     prefix |= U(s_bin) << shift;
@@ -531,6 +558,44 @@ __global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) topk_gather_kernel(co
   const int64_t stride = int64_t(gridDim.x) * SEL_NT;
   const int64_t gtid = int64_t(blockIdx.x) * SEL_NT + threadIdx.x;
   for (int64_t j = greater + gtid; j < k; j += stride) out[j] = vraw;
+}
+
+// ---- sort of a small top-k output in one CTA ------------------------------------------
+// The k <= topk_small_sort_max<U>() outputs are sorted ascending by their ordered value in shared
+// memory (a bitonic network over the next power of two, padded with the largest ordered value,
+// so the padding sorts behind every key and only the first k slots are written back).  Keys
+// with equal ordered values have equal bits, so the bytes equal the LSD sort's.
+template <class U>
+__host__ __device__ constexpr int topk_small_sort_max() {
+  return sizeof(U) == 4 ? 8192 : 4096;  // 32 KiB of shared memory
+}
+constexpr int TOPK_SMALL_SORT_NT = 1024;
+
+template <class U, int KIND>
+__global__ void __launch_bounds__(TOPK_SMALL_SORT_NT) topk_small_sort_kernel(U* __restrict__ out, int k) {
+  using KO = KeyOrder<U, KIND>;
+  __shared__ U s[topk_small_sort_max<U>()];
+  if (k <= 1) return;
+  int N = 2;
+  while (N < k) N <<= 1;
+  for (int i = threadIdx.x; i < N; i += TOPK_SMALL_SORT_NT) s[i] = i < k ? KO::to_ordered(out[i]) : U(~U(0));
+  __syncthreads();
+  for (int size = 2; size <= N; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int p = threadIdx.x; p < (N >> 1); p += TOPK_SMALL_SORT_NT) {
+        const int i = ((p & ~(stride - 1)) << 1) | (p & (stride - 1));  // lower element of the pair
+        const int j = i + stride;
+        const bool up = (i & size) == 0;
+        const U a = s[i], b = s[j];
+        if ((a > b) == up) {
+          s[i] = b;
+          s[j] = a;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = threadIdx.x; i < k; i += TOPK_SMALL_SORT_NT) out[i] = KO::from_ordered(s[i]);
 }
 
 }  // namespace hpcs

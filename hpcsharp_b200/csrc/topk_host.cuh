@@ -76,29 +76,35 @@ inline int topk_largest_enqueue(hpcs_ctx* ctx, const U* d, int64_t n, int64_t k,
   SelectState* st = static_cast<SelectState*>(ctx->aux1.ptr);
   U* cand = static_cast<U*>(ctx->aux0.ptr);
   const int grid = select_grid(ctx, n, int(sizeof(U)));
+  // sampled keys expected at or above the threshold: enough that fewer than k candidates
+  // (k keys sampled at rate S/n, Poisson) is many standard deviations away
+  constexpr int S = topk_sample_size<U>();
+  const double ks = double(k) * S / double(n);
+  const int64_t m = int64_t(1.5 * ks + 6.0 * std::sqrt(ks) + 8.0) + 1;
+  // the passes over the candidates get a grid for about twice the expected number (m / S of
+  // the keys; all of them below the sampling size); any number is correct, more take longer
+  const int64_t expect = n < int64_t(4) * S || m >= S ? n : int64_t(double(m) / S * double(n)) + k;
+  const int cgrid = select_grid(ctx, 2 * expect, int(sizeof(U)));
   {
     KernelTimer kt(ctx, s, HPCS_K_TOPK);
-    select_init_kernel<<<1, 256, 0, s>>>(st, n - k, n);
-    // sampled keys expected at or above the threshold: enough that fewer than k candidates
-    // (k keys sampled at rate S/n, Poisson) is many standard deviations away
-    const double ks = double(k) * TOPK_SAMPLE / double(n);
-    const int64_t m = int64_t(1.5 * ks + 6.0 * std::sqrt(ks) + 8.0) + 1;
-    topk_sample_kernel<U, KIND><<<1, TOPK_SAMPLE_NT, 0, s>>>(d, n, m, st);
+    topk_sample_kernel<U, KIND><<<1, TOPK_SAMPLE_NT, 0, s>>>(d, n, k, m, st);
     topk_filter_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, cand, st);
     topk_decide_kernel<<<1, 32, 0, s>>>(st, n, k);
     // level 0: over the candidates, or (fallback) over all keys with the compaction
-    select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(cand, &st->cand_count, 0, st, BITS - 8, SEL_MODE_CAND);
+    select_hist_kernel<U, KIND><<<cgrid, SEL_NT, 0, s>>>(cand, &st->cand_count, 0, st, BITS - 8, SEL_MODE_CAND);
     select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, nullptr, n, st, BITS - 8, SEL_MODE_FULL);
     select_pick_kernel<U><<<1, 256, 0, s>>>(st, BITS - 8, LEVELS == 1);
     select_compact_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, cand, st, out, k, SEL_MODE_FULL);
     for (int l = 1; l < LEVELS; l++) {
       const int shift = BITS - 8 * (l + 1);
-      select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(cand, &st->cand_count, 0, st, shift);
+      select_hist_kernel<U, KIND><<<cgrid, SEL_NT, 0, s>>>(cand, &st->cand_count, 0, st, shift);
       select_pick_kernel<U><<<1, 256, 0, s>>>(st, shift, l == LEVELS - 1);
     }
-    topk_gather_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(cand, k, st, out);
+    topk_gather_kernel<U, KIND><<<cgrid, SEL_NT, 0, s>>>(cand, k, st, out);
+    if (k <= topk_small_sort_max<U>()) topk_small_sort_kernel<U, KIND><<<1, TOPK_SMALL_SORT_NT, 0, s>>>(out, int(k));
     HPCS_CUDA(cudaGetLastError());
   }
+  if (k <= topk_small_sort_max<U>()) return HPCS_OK;
   return enqueue_sort<U, KIND, NoValue>(ctx, out, nullptr, k, s);
 }
 

@@ -75,7 +75,9 @@ class HpcsConfig(C.Structure):
         ("poison_tile", C.c_int32),
         ("pass_scheme", C.c_int32),
         ("staged_host_copies", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("seg_grid_min_keys", C.c_int32),
+        ("seg_grid_tiles", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -252,10 +254,13 @@ class Context:
 
     def __init__(self, device: int = 0, *, pool_bytes: int = 0, skip_trivial_passes: bool = True,
                  spin_limit_ns: int = 2_000_000_000, poison_tile: int = -1, rank_mode: int = 0,
-                 pass_scheme: str = "auto", staged_host_copies: bool = True):
+                 pass_scheme: str = "auto", staged_host_copies: bool = True, seg_grid_min_keys: int = 0,
+                 seg_grid_tiles: int = 0):
         self.lib = load()
         cfg = default_config()
         cfg.staged_host_copies = 1 if staged_host_copies else 0
+        cfg.seg_grid_min_keys = seg_grid_min_keys
+        cfg.seg_grid_tiles = seg_grid_tiles
         cfg.pool_bytes = pool_bytes
         cfg.skip_trivial_passes = 1 if skip_trivial_passes else 0
         cfg.spin_limit_ns = spin_limit_ns

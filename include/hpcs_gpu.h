@@ -87,7 +87,12 @@ typedef struct hpcs_config {
                                   the context's pinned buffers in chunks, several host threads
                                   copying while the DMA engine moves earlier chunks; 0: one
                                   cudaMemcpyAsync per array (the driver stages it) */
-  int32_t reserved[5];
+  int32_t seg_grid_min_keys;   /* batched sort: arrays of at least this many keys (16-byte
+                                  aligned) take the plain sort's kernels, spread over
+                                  several CTAs each; 0 = 65536, negative = never */
+  int32_t seg_grid_tiles;      /* batched sort: 16 Ki-key tiles per CTA of such an array
+                                  (0 = 32) */
+  int32_t reserved[3];
 } hpcs_config;
 
 /* ---- context ---------------------------------------------------------------------- */

@@ -186,16 +186,23 @@ def test_builtin_table_is_the_tuned_record(ctx):
     assert ctx.seg_tuning == rec["table"]
 
 
-GRID_LENGTHS = [262_144, 262_145, 16_384 * 8 * 3 - 1, 1_048_576 + 7, 2_500_001]
+GRID_LENGTHS = [65_536, 100_003, 262_145, 16_384 * 8 * 3 - 1, 1_048_576 + 7, 2_500_001]
+# (minimum length, tiles per CTA): the defaults (65,536 and 32), and 2^18 keys with 8-tile
+# ranges, where every array of the grid level spans several CTAs
+GRID_GEOMETRIES = [(0, 0), (262_144, 8)]
 
 
+@pytest.mark.parametrize("geometry", GRID_GEOMETRIES, ids=["default", "min256k_tiles8"])
 @pytest.mark.parametrize("use_plan", [False, True], ids=["one_shot", "plan_twice"])
-def test_grid_level_arrays(ctx, orc, use_plan):
-    """Arrays of at least 2^18 aligned keys go to the grid-level path (many CTAs per array, the
-    plain sort's kernels per range); unaligned ones of the same length stay on the block-level
-    path.  Constant and low-byte-only arrays make passes the identity (an odd number runs: the
-    copy back).  Every array must equal the oracle's sort of it alone."""
+def test_grid_level_arrays(ctx, orc, use_plan, geometry):
+    """Arrays of at least the context's grid-level length, with aligned keys, go to the grid
+    level (the plain sort's kernels per range of the array); unaligned ones of the same length
+    stay on the block level.  Constant and low-byte-only arrays make passes the identity (an odd
+    number runs: the copy back).  Every array must equal the oracle's sort of it alone."""
     import torch
+
+    if geometry != (0, 0):
+        ctx = native.Context(0, seg_grid_min_keys=geometry[0], seg_grid_tiles=geometry[1])
 
     host = []
     for i, n in enumerate(GRID_LENGTHS):
@@ -228,3 +235,5 @@ def test_grid_level_arrays(ctx, orc, use_plan):
         torch.cuda.synchronize()
         ctx.synchronize()
         check(host, devs, orc)
+    if geometry != (0, 0):
+        ctx.close()
