@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) select_compact_kernel
 // the kernels of the path not taken return at their first instruction.
 template <class U>
 __host__ __device__ constexpr int topk_sample_size() {
-  return sizeof(U) == 4 ? 32768 : 16384;  // 32 / 16 keys per thread in registers
+  return 8192;  // 8 keys per thread in registers
 }
 constexpr int TOPK_SAMPLE_NT = 1024;
 
@@ -383,60 +383,76 @@ __global__ void __launch_bounds__(PART_NT) partition_count_kernel(const U* __res
   if (threadIdx.x < 3) tile_counts[int64_t(blockIdx.x) * 3 + threadIdx.x] = c[threadIdx.x];
 }
 
-// One block: tile_counts[t][c] -> exclusive start of tile t's class-c keys in the output.
-// Each thread takes PART_SCAN_PER consecutive tiles per step.
-constexpr int PART_SCAN_PER = 4;
-static __global__ void partition_scan_kernel(uint32_t* tile_counts, int64_t tiles, const SelectState* st, int64_t n) {
-  __shared__ int64_t carry[3];
-  __shared__ int64_t wsum[3][32];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;  // 1024 threads
-  if (tid < 3) {
-    const int64_t less = st->less, eq = st->eq;
-    carry[tid] = tid == 0 ? 0 : (tid == 1 ? less : less + eq);
+// Scan of the per-tile class counts in two levels: partition_block_scan_kernel turns the
+// counts of each run of 1024 tiles into starts within the run and records the run's totals;
+// partition_top_scan_kernel (one CTA) turns the run totals into run starts, class c's run
+// starting after all keys of the classes below it (st->less, st->eq).  A tile's start is its
+// run's start plus its start within the run.  (A single CTA stepping through all tiles took
+// 109-143 us for 65,536 tiles.)
+constexpr int PART_SCAN_RUN = 1024;
+
+template <int NT>
+__device__ __forceinline__ void block_exclusive_scan3(const uint32_t (&v)[3], uint32_t (&excl)[3], uint32_t (&total)[3],
+                                                      uint32_t (*wsum)[NT / 32]) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t incl[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    incl[c] = v[c];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl[c], o);
+      if (lane >= o) incl[c] += y;
+    }
+    if (lane == 31) wsum[c][warp] = incl[c];
   }
   __syncthreads();
-  for (int64_t b0 = 0; b0 < tiles; b0 += 1024 * PART_SCAN_PER) {
-    const int64_t t0 = b0 + int64_t(tid) * PART_SCAN_PER;
-    uint32_t v[3][PART_SCAN_PER];
-    int64_t sum[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-      sum[c] = 0;
-#pragma unroll
-      for (int q = 0; q < PART_SCAN_PER; q++) {
-        v[c][q] = t0 + q < tiles ? tile_counts[(t0 + q) * 3 + c] : 0u;
-        sum[c] += v[c][q];
-      }
+  for (int c = 0; c < 3; c++) {
+    uint32_t before = 0, all = 0;
+    for (int w = 0; w < NT / 32; w++) {
+      const uint32_t x = wsum[c][w];
+      before += w < warp ? x : 0u;
+      all += x;
     }
-    int64_t incl[3];
+    excl[c] = before + incl[c] - v[c];
+    total[c] = all;
+  }
+}
+
+static __global__ void __launch_bounds__(PART_SCAN_RUN) partition_block_scan_kernel(uint32_t* tile_counts, int64_t tiles,
+                                                                                   uint32_t* run_totals) {
+  __shared__ uint32_t wsum[3][PART_SCAN_RUN / 32];
+  const int64_t t = int64_t(blockIdx.x) * PART_SCAN_RUN + threadIdx.x;
+  uint32_t v[3] = {0u, 0u, 0u}, excl[3], total[3];
+  if (t < tiles) {
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-      incl[c] = sum[c];
+    for (int c = 0; c < 3; c++) v[c] = tile_counts[t * 3 + c];
+  }
+  block_exclusive_scan3<PART_SCAN_RUN>(v, excl, total, wsum);
+  if (t < tiles) {
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int64_t y = __shfl_up_sync(0xFFFFFFFFu, incl[c], o);
-        if (lane >= o) incl[c] += y;
-      }
-      if (lane == 31) wsum[c][warp] = incl[c];
-    }
-    __syncthreads();
+    for (int c = 0; c < 3; c++) tile_counts[t * 3 + c] = excl[c];
+  }
+  if (threadIdx.x < 3) run_totals[int64_t(blockIdx.x) * 3 + threadIdx.x] = total[threadIdx.x];
+}
+
+// runs <= 1024 (n < 2^31 keys in 4096-key tiles is at most 512 runs)
+static __global__ void __launch_bounds__(1024) partition_top_scan_kernel(uint32_t* run_totals, int runs,
+                                                                         const SelectState* st) {
+  __shared__ uint32_t wsum[3][32];
+  const int r = threadIdx.x;
+  uint32_t v[3] = {0u, 0u, 0u}, excl[3], total[3];
+  if (r < runs) {
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-      int64_t run = carry[c] + incl[c] - sum[c];
-      for (int w = 0; w < warp; w++) run += wsum[c][w];
-#pragma unroll
-      for (int q = 0; q < PART_SCAN_PER; q++) {
-        if (t0 + q < tiles) tile_counts[(t0 + q) * 3 + c] = uint32_t(run);
-        run += v[c][q];
-      }
-    }
-    __syncthreads();
-    if (tid < 3) {
-      int64_t tot = 0;
-      for (int w = 0; w < 32; w++) tot += wsum[tid][w];
-      carry[tid] += tot;
-    }
-    __syncthreads();
+    for (int c = 0; c < 3; c++) v[c] = run_totals[r * 3 + c];
+  }
+  block_exclusive_scan3<1024>(v, excl, total, wsum);
+  const uint32_t less = uint32_t(st->less), eq = uint32_t(st->eq);
+  if (r < runs) {
+    run_totals[r * 3 + 0] = excl[0];
+    run_totals[r * 3 + 1] = less + excl[1];
+    run_totals[r * 3 + 2] = less + eq + excl[2];
   }
 }
 
@@ -448,6 +464,7 @@ template <class U, int KIND>
 __global__ void __launch_bounds__(PART_NT) partition_scatter_kernel(const U* __restrict__ keys, int64_t n,
                                                                     const SelectState* st,
                                                                     const uint32_t* tile_starts,
+                                                                    const uint32_t* run_starts,
                                                                     U* __restrict__ out) {
   constexpr int E = int(16 / sizeof(U));
   static_assert(PART_KPT % E == 0, "whole vectors per thread");
@@ -526,7 +543,8 @@ __global__ void __launch_bounds__(PART_NT) partition_scatter_kernel(const U* __r
   __syncthreads();
   const uint32_t at1 = s_at[1], at2 = s_at[2];
   const uint32_t* ts = tile_starts + int64_t(blockIdx.x) * 3;
-  const int64_t o0 = ts[0], o1 = int64_t(ts[1]) - at1, o2 = int64_t(ts[2]) - at2;
+  const uint32_t* rs = run_starts + int64_t(blockIdx.x / PART_SCAN_RUN) * 3;
+  const int64_t o0 = int64_t(rs[0]) + ts[0], o1 = int64_t(rs[1]) + ts[1] - at1, o2 = int64_t(rs[2]) + ts[2] - at2;
   for (int j = tid; j < tile_n; j += PART_NT) {
     const uint32_t uj = uint32_t(j);
     const int64_t pos = (uj < at1 ? o0 : (uj < at2 ? o1 : o2)) + j;
