@@ -25,8 +25,11 @@
 //   reorder  keys into shared memory in (digit, input order) order;
 //   scatter  coalesced per-digit runs to global memory, and the next-digit count.
 //
-// Next-digit counters are 16 bits, two per word, J x 256 of them (74 KiB for J = 148).  A
-// counter that reaches 0x8000 is moved to the global table by the thread whose increment
+// Next-digit counters are 16 bits, J x 256 of them (74 KiB for J = 148), two per word: word
+// (q / 2) * 256 + e holds range q's counter of next digit e in its low half for even q and in
+// its high half for odd q.  The keys of a warp instruction mostly land in one range, so their
+// random digits spread over 256 words (measured on B200: ~4 clocks per random warp atomic on 256
+// words, ~6 on 128 words, where pairs of digits share a word).  A counter that reaches 0x8000 is moved to the global table by the thread whose increment
 // reached it (it subtracts 0x8000 in shared memory and adds 0x8000 in global memory).  One
 // increment per key, so exactly one thread sees each crossing, and between a crossing and
 // its subtraction at most one tile of other increments can land (each thread's subtraction
@@ -53,18 +56,21 @@ struct ChunkSmem {
   static constexpr size_t OFF_MSK = OFF_CNT + size_t(NW) * RS * 4;
   static constexpr size_t MSK_BYTES = MODE == RANK_PEER_MASK ? size_t(NW) * 2 * RADIX * 4 : 0;
   static constexpr size_t OFF_RUN = (OFF_MSK + MSK_BYTES + 15) / 16 * 16;  // running start per digit
-  // per digit for this tile: {global base, next-digit counter row of its first key's range,
-  // first position of the following range, 0}
+  // per digit for this tile: {global base, counter words of its first key's range q (word base
+  // | half << 31), first position of range q + 1, counter words of range q + 1}
   static constexpr size_t OFF_META = OFF_RUN + RADIX * 4;
   static constexpr size_t OFF_WSUM = OFF_META + RADIX * 16;
   static constexpr size_t OFF_MBAR = (OFF_WSUM + 32 * 4 + 7) / 8 * 8;
-  static constexpr size_t OFF_CTAB = (OFF_MBAR + 16 + 15) / 16 * 16;  // [J][128] words
+  static constexpr size_t OFF_CTAB = (OFF_MBAR + 16 + 15) / 16 * 16;  // [(J + 1) / 2][256] words
   static constexpr size_t BASE_BYTES = OFF_CTAB;
-  static constexpr size_t bytes(int chunks) { return BASE_BYTES + size_t(chunks) * (RADIX / 2) * 4; }
+  static constexpr size_t bytes(int chunks) { return BASE_BYTES + size_t((chunks + 1) / 2) * RADIX * 4; }
   static_assert(TILE <= 16384, "16-bit next-digit counters assume at most 16384 keys per tile");
   static_assert(G >= 1 && (G & (G - 1)) == 0 && NW % G == 0 && 32 % NW == 0, "digit-scan geometry");
   static_assert(size_t(NW) * RS >= size_t(G) * RADIX, "prologue partials fit in the counters");
 };
+
+// Counter words of range q in the next-digit table: word base (q / 2) * 256, half q % 2 in bit 31.
+__device__ __forceinline__ uint32_t ctab_words(uint32_t q) { return (q >> 1) * uint32_t(RADIX) | ((q & 1u) << 31); }
 
 // Ranks of one warp's keys are turned into tile offsets by a scan over (digit, warp) in
 // which every thread takes part: thread t handles digit t / G and the NWG consecutive warps
@@ -141,7 +147,7 @@ __device__ __forceinline__ void chunk_pass_body(const SortArgs& args, const int 
   }
   for (int i = tid; i < RADIX; i += NT) czero[int64_t(j) * RADIX + i] = 0u;
   if (nshift >= 0)
-    for (int i = tid; i < J * (RADIX / 2); i += NT) s_ctab[i] = 0u;
+    for (int i = tid; i < (J + 1) / 2 * RADIX; i += NT) s_ctab[i] = 0u;
   if (MODE == RANK_PEER_MASK)
     for (int i = lane; i < 2 * RADIX; i += 32) msk_w[i] = 0u;
 
@@ -307,7 +313,7 @@ __device__ __forceinline__ void chunk_pass_body(const SortArgs& args, const int 
         const uint32_t r = s_run[sd];
         uint32_t q = __umulhi(r, magic);
         q -= (q * LK > r) ? 1u : 0u;
-        s_meta[sd] = make_uint4(r - local, q * (RADIX / 2), (q + 1u) * LK, 0u);
+        s_meta[sd] = make_uint4(r - local, ctab_words(q), (q + 1u) * LK, ctab_words(q + 1u));
         s_run[sd] = r + total;
       }
     }
@@ -357,9 +363,9 @@ __device__ __forceinline__ void chunk_pass_body(const SortArgs& args, const int 
           kout_base[pos] = k;
           const uint32_t e = ndig(k);
           if (nshift >= 0 && !next_skewed && e != next_heavy) {
-            const uint32_t row = m.y + (pos >= m.z ? uint32_t(RADIX / 2) : 0u);
-            const uint32_t inc = 1u + (e & 1u) * 0xFFFFu;
-            const uint32_t old = atomicAdd(s_ctab + row + (e >> 1), inc);
+            const uint32_t cw = pos >= m.z ? m.w : m.y;
+            const uint32_t inc = 1u << ((cw >> 31) << 4);
+            const uint32_t old = atomicAdd(s_ctab + (cw & 0x7FFFFFFFu) + e, inc);
             // a half went from 0x7FFF to 0x8000 (the other half is unchanged)
             if ((old + inc) & ~old & 0x80008000u) crossed |= 1u << i;
           }
@@ -376,11 +382,11 @@ __device__ __forceinline__ void chunk_pass_body(const SortArgs& args, const int 
         const uint32_t e = ndig(k);
         const uint4 m = s_meta[dig(k)];
         const uint32_t pos = m.x + uint32_t(s);
-        const uint32_t row = m.y + (pos >= m.z ? uint32_t(RADIX / 2) : 0u);
+        const uint32_t cw = pos >= m.z ? m.w : m.y;
         const bool counted = (FULL || s < tile_n) && pos < n32 && e != next_heavy;
-        const uint32_t word = row + (e >> 1);
-        const uint32_t unit = 1u + (e & 1u) * 0xFFFFu;
-        const uint32_t code = (word << 1) | (e & 1u);
+        const uint32_t word = (cw & 0x7FFFFFFFu) + e;
+        const uint32_t unit = 1u << ((cw >> 31) << 4);
+        const uint32_t code = (word << 1) | (cw >> 31);
         const uint32_t lanes = __ballot_sync(0xFFFFFFFFu, counted);
         if (lanes == 0u) continue;
         const int leader = __ffs(lanes) - 1;
@@ -403,11 +409,12 @@ __device__ __forceinline__ void chunk_pass_body(const SortArgs& args, const int 
           const U k = key[i];
           const uint4 m = s_meta[dig(k)];
           const uint32_t pos = m.x + uint32_t(s);
-          const uint32_t row = m.y + (pos >= m.z ? uint32_t(RADIX / 2) : 0u);
+          const uint32_t cw = pos >= m.z ? m.w : m.y;
           const uint32_t e = ndig(k);
-          const uint32_t sh = (e & 1u) << 4;
-          atomicSub(s_ctab + row + (e >> 1), 0x8000u << sh);
-          atomicAdd(cout + 2u * row + e, 0x8000u);
+          const uint32_t sh = (cw >> 31) << 4;
+          const uint32_t q = ((cw & 0x7FFFFFFFu) / RADIX) * 2u + (cw >> 31);  // the range
+          atomicSub(s_ctab + (cw & 0x7FFFFFFFu) + e, 0x8000u << sh);
+          atomicAdd(cout + q * RADIX + e, 0x8000u);
         }
       }
     }
@@ -457,10 +464,11 @@ __device__ __forceinline__ void chunk_pass_body(const SortArgs& args, const int 
   // add this CTA's next-digit counts into the global table (nonzero counters only)
   if (nshift >= 0) {
     __syncthreads();
-    for (int i = tid; i < J * (RADIX / 2); i += NT) {
+    for (int i = tid; i < (J + 1) / 2 * RADIX; i += NT) {
       const uint32_t v = s_ctab[i];
-      if (v & 0xFFFFu) atomicAdd(cout + 2 * i, v & 0xFFFFu);
-      if (v >> 16) atomicAdd(cout + 2 * i + 1, v >> 16);
+      const int e = i % RADIX, q0 = (i / RADIX) * 2;  // ranges q0 (low half) and q0 + 1
+      if (v & 0xFFFFu) atomicAdd(cout + q0 * RADIX + e, v & 0xFFFFu);
+      if (v >> 16) atomicAdd(cout + (q0 + 1) * RADIX + e, v >> 16);
     }
   }
 }

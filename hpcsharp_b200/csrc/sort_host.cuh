@@ -218,7 +218,7 @@ struct ChunkShape {
   using C = ChunkConfig<U, V, MODE>;
   using L = ChunkSmem<U, V, C::NT, C::KPT, MODE>;
   static constexpr int TILE = L::TILE;
-  static constexpr int MAX_RANGES = int((MAX_DYN_SMEM - L::BASE_BYTES) / ((RADIX / 2) * 4));
+  static constexpr int MAX_RANGES = 2 * int((MAX_DYN_SMEM - L::BASE_BYTES) / (RADIX * 4));
 };
 
 constexpr int HIST_NT = 1024;
