@@ -81,12 +81,19 @@ __global__ void __launch_bounds__(COUNT_NT) count_hist_kernel(const T* __restric
     const uint4* vp = reinterpret_cast<const uint4*>(a + head);
     const int64_t G = int64_t(gridDim.x) * COUNT_NT;
     const int64_t gtid = int64_t(blockIdx.x) * COUNT_NT + tid;
+    // the next round's vectors are loaded before this round's keys are counted, so two rounds
+    // of loads are in flight (one round alone left the loop waiting on memory)
+    Vec v[VPR], vn[VPR];
+#pragma unroll
+    for (int j = 0; j < VPR; j++) {
+      const int64_t idx = j * G + gtid;
+      v[j].v = idx < nvec ? __ldg(vp + idx) : make_uint4(0u, 0u, 0u, 0u);
+    }
     for (int64_t base = 0; base < nvec; base += G * VPR) {  // the same number of rounds in every thread
-      Vec v[VPR];
 #pragma unroll
       for (int j = 0; j < VPR; j++) {
-        const int64_t idx = base + j * G + gtid;
-        v[j].v = idx < nvec ? __ldg(vp + idx) : make_uint4(0u, 0u, 0u, 0u);
+        const int64_t idx = base + G * VPR + j * G + gtid;
+        vn[j].v = idx < nvec ? __ldg(vp + idx) : make_uint4(0u, 0u, 0u, 0u);
       }
 #pragma unroll
       for (int j = 0; j < VPR; j++)
@@ -95,6 +102,8 @@ __global__ void __launch_bounds__(COUNT_NT) count_hist_kernel(const T* __restric
           for (int e = 0; e < E; e++) bump(uint32_t(v[j].k[e]));
         }
       __syncthreads();
+#pragma unroll
+      for (int j = 0; j < VPR; j++) v[j] = vn[j];
     }
     if (blockIdx.x == 0 && tid == 0) {  // fewer than 2E keys outside the vectors
       for (int64_t i = 0; i < head; i++) bump(uint32_t(a[i]));
