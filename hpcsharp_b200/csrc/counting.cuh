@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(COUNT_NT) count_hist_kernel(const T* __restric
   if (BINS == 256) {
     for (int i = tid; i < 256 * 32; i += COUNT_NT) sh[i] = 0u;
     __syncthreads();
-    visit_keys<T, 2>(a, n, [&](const T* k, int nv) {
+    visit_keys<T, 4>(a, n, [&](const T* k, int nv) {
 #pragma unroll
       for (int e = 0; e < E; e++)
         if (e < nv) atomicAdd(&sh[((uint32_t(k[e]) ^ flip) & 0xFFu) * 32 + lane], 1u);

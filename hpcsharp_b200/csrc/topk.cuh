@@ -37,29 +37,15 @@ struct SelectState {
   int64_t cand_count;  // candidates compacted after level 0
   unsigned long long gathered;  // keys > v written to the top-k output so far
   int64_t n_total;     // keys selected among
-  uint64_t threshold;  // top-k: ordered keys at or above it are the filter's candidates
-  int32_t mode;        // top-k: SEL_MODE_CAND (select among the candidates) or SEL_MODE_FULL
+  uint64_t threshold;  // top-k: ordered keys at or above it are the filter's candidates;
+                       // select: the window's lower end
+  uint64_t threshold_hi;        // select: the window's upper end (inclusive)
+  unsigned long long below;     // select: keys below the window
+  int32_t mode;        // SEL_MODE_CAND (select among the candidates) or SEL_MODE_FULL
   int32_t pad;
   uint32_t hist[256];
 };
 enum : int32_t { SEL_MODE_ANY = -1, SEL_MODE_FULL = 0, SEL_MODE_CAND = 1 };
-
-static __global__ void select_init_kernel(SelectState* st, int64_t rank, int64_t n) {
-  const int tid = threadIdx.x;
-  if (tid == 0) {
-    st->n_total = n;
-    st->prefix = 0;
-    st->mask = 0;
-    st->rank = rank;
-    st->less = 0;
-    st->eq = 0;
-    st->cand_count = 0;
-    st->gathered = 0;
-    st->threshold = 0;
-    st->mode = SEL_MODE_FULL;
-  }
-  if (tid < 256) st->hist[tid] = 0;
-}
 
 constexpr int SEL_NT = 512;
 constexpr int SEL_COPIES = 32;
@@ -234,43 +220,14 @@ __host__ __device__ constexpr int topk_sample_size() {
 }
 constexpr int TOPK_SAMPLE_NT = 1024;
 
-// One CTA: the SelectState set up for the k largest of n keys (rank n - k), and the ordered
-// sample value of rank (S - m) among S = topk_sample_size<U>() keys at stride n / S, by an MSD
-// radix select in shared memory (per level a histogram of the samples matching the prefix and
-// a scan of its 256 bins by 8 warps).  Writes st->threshold (0 = keep every key).
-template <class U, int KIND>
-__global__ void __launch_bounds__(TOPK_SAMPLE_NT) topk_sample_kernel(const U* __restrict__ keys, int64_t n,
-                                                                     int64_t k, int64_t m, SelectState* st) {
-  using KO = KeyOrder<U, KIND>;
+// The ordered value of 0-based ascending rank `rank` among the TOPK_SAMPLE_NT x PER samples o[]
+// held by the CTA's threads: an MSD radix select in shared memory, per level a histogram of the
+// samples matching the prefix and a scan of its 256 bins by 8 warps.  Every thread returns it.
+template <class U, int PER>
+__device__ __forceinline__ U sample_rank_value(const U (&o)[PER], uint32_t rank, uint32_t* hist, uint32_t* s_wsum,
+                                               uint32_t* s_pick) {
   constexpr int BITS = int(sizeof(U) * 8);
-  constexpr int S = topk_sample_size<U>();
-  constexpr int PER = S / TOPK_SAMPLE_NT;
-  __shared__ uint32_t hist[256];
-  __shared__ uint32_t s_wsum[8];
-  __shared__ uint32_t s_bin, s_below;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0) {
-    st->n_total = n;
-    st->prefix = 0;
-    st->mask = 0;
-    st->rank = n - k;
-    st->less = 0;
-    st->eq = 0;
-    st->cand_count = 0;
-    st->gathered = 0;
-    st->mode = SEL_MODE_FULL;
-  }
-  if (tid < 256) st->hist[tid] = 0;
-  if (n < int64_t(4) * S || m >= S) {  // too few keys to sample: keep them all
-    if (tid == 0) st->threshold = 0;
-    return;
-  }
-  const int64_t stride = n / S;
-  U o[PER];
-#pragma unroll
-  for (int q = 0; q < PER; q++) o[q] = KO::to_ordered(keys[int64_t(tid + q * TOPK_SAMPLE_NT) * stride]);
-  // rank (0-based, ascending) of the threshold among the samples
-  uint32_t rank = uint32_t(S - m);
   U prefix = 0, mask = 0;
   for (int shift = BITS - 8; shift >= 0; shift -= 8) {
     if (tid < 256) hist[tid] = 0;
@@ -297,17 +254,156 @@ __global__ void __launch_bounds__(TOPK_SAMPLE_NT) topk_sample_kernel(const U* __
       const uint32_t excl = base + incl - c;
       // the bins' ranges [excl, excl + c) are disjoint: exactly one thread matches
       if ((c > 0u && rank >= excl && rank < excl + c) || (tid == 255 && rank >= excl + c)) {
-        s_bin = uint32_t(tid);
-        s_below = excl;
+        s_pick[0] = uint32_t(tid);
+        s_pick[1] = excl;
       }
     }
     __syncthreads();
-    prefix |= U(s_bin) << shift;
+    prefix |= U(s_pick[0]) << shift;
     mask |= U(0xFF) << shift;
-    rank -= s_below;
+    rank -= s_pick[1];
     __syncthreads();
   }
-  if (tid == 0) st->threshold = uint64_t(prefix);
+  return prefix;
+}
+
+// One CTA: the SelectState set up for the k largest of n keys (rank n - k), and the ordered
+// sample value of rank (S - m) among S = topk_sample_size<U>() keys at stride n / S.  Writes
+// st->threshold (0 = keep every key).
+template <class U, int KIND>
+__global__ void __launch_bounds__(TOPK_SAMPLE_NT) topk_sample_kernel(const U* __restrict__ keys, int64_t n,
+                                                                     int64_t k, int64_t m, SelectState* st) {
+  using KO = KeyOrder<U, KIND>;
+  constexpr int S = topk_sample_size<U>();
+  constexpr int PER = S / TOPK_SAMPLE_NT;
+  __shared__ uint32_t hist[256];
+  __shared__ uint32_t s_wsum[8];
+  __shared__ uint32_t s_pick[2];
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    st->n_total = n;
+    st->prefix = 0;
+    st->mask = 0;
+    st->rank = n - k;
+    st->less = 0;
+    st->eq = 0;
+    st->cand_count = 0;
+    st->gathered = 0;
+    st->below = 0;
+    st->mode = SEL_MODE_FULL;
+  }
+  if (tid < 256) st->hist[tid] = 0;
+  if (n < int64_t(4) * S || m >= S) {  // too few keys to sample: keep them all
+    if (tid == 0) st->threshold = 0;
+    return;
+  }
+  const int64_t stride = n / S;
+  U o[PER];
+#pragma unroll
+  for (int q = 0; q < PER; q++) o[q] = KO::to_ordered(keys[int64_t(tid + q * TOPK_SAMPLE_NT) * stride]);
+  const U t = sample_rank_value<U, PER>(o, uint32_t(S - m), hist, s_wsum, s_pick);
+  if (tid == 0) st->threshold = uint64_t(t);
+}
+
+// ---- radix select with one read of the keys ---------------------------------------------
+// The key of rank r among n: the same strided sample gives two values lo <= hi whose sample
+// ranks lie m below and m above r's expected sample rank (r S / n); one read counts the keys
+// below lo and keeps the keys in [lo, hi] (the candidates).  When r falls among the candidates
+// (below <= r < below + candidates), the radix select runs over the candidates only, with
+// `below` keys already counted under the prefix; otherwise over all keys (the two-read path).
+// The choice is made on the device, as for the k largest.
+
+// One CTA: the SelectState set up for rank `rank` among n keys, and the window [lo, hi].  An
+// input too small to sample gets an empty window (lo > hi), which sends the select to the
+// two-read path.
+template <class U, int KIND>
+__global__ void __launch_bounds__(TOPK_SAMPLE_NT) select_sample_kernel(const U* __restrict__ keys, int64_t n,
+                                                                       int64_t rank, int64_t m, SelectState* st) {
+  using KO = KeyOrder<U, KIND>;
+  constexpr int S = topk_sample_size<U>();
+  constexpr int PER = S / TOPK_SAMPLE_NT;
+  __shared__ uint32_t hist[256];
+  __shared__ uint32_t s_wsum[8];
+  __shared__ uint32_t s_pick[2];
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    st->n_total = n;
+    st->prefix = 0;
+    st->mask = 0;
+    st->rank = rank;
+    st->less = 0;
+    st->eq = 0;
+    st->cand_count = 0;
+    st->gathered = 0;
+    st->below = 0;
+    st->mode = SEL_MODE_FULL;
+  }
+  if (tid < 256) st->hist[tid] = 0;
+  if (n < int64_t(4) * S) {
+    if (tid == 0) {
+      st->threshold = 1;
+      st->threshold_hi = 0;
+    }
+    return;
+  }
+  const int64_t stride = n / S;
+  U o[PER];
+#pragma unroll
+  for (int q = 0; q < PER; q++) o[q] = KO::to_ordered(keys[int64_t(tid + q * TOPK_SAMPLE_NT) * stride]);
+  const int64_t rs = rank * S / n;  // expected sample rank of the selected key
+  const int64_t rlo = rs - m, rhi = rs + m;
+  // the window reaches the ends of the key range where the margin passes the sample's ends
+  const U lo = rlo <= 0 ? U(0) : sample_rank_value<U, PER>(o, uint32_t(rlo), hist, s_wsum, s_pick);
+  const U hi = rhi >= S - 1 ? U(~U(0)) : sample_rank_value<U, PER>(o, uint32_t(rhi), hist, s_wsum, s_pick);
+  if (tid == 0) {
+    st->threshold = uint64_t(lo);
+    st->threshold_hi = uint64_t(hi);
+  }
+}
+
+// One read of the keys: keys in [lo, hi] go to `cand`, keys below lo are counted.
+template <class U, int KIND>
+__global__ void __launch_bounds__(SEL_NT, SEL_CTAS_PER_SM) select_window_kernel(const U* __restrict__ keys, int64_t n,
+                                                                               U* __restrict__ cand, SelectState* st) {
+  using KO = KeyOrder<U, KIND>;
+  constexpr int E = int(16 / sizeof(U));
+  constexpr int CAP = 1024 / int(sizeof(U));
+  __shared__ U s_buf[SEL_NT / 32][CAP];
+  const U lo = U(st->threshold), hi = U(st->threshold_hi);
+  WarpStage<U, E, CAP> to_cand{s_buf[threadIdx.x >> 5], 0u, cand,
+                               reinterpret_cast<unsigned long long*>(&st->cand_count), INT64_MAX};
+  uint32_t below = 0;
+  visit_keys<U, SEL_VPT>(keys, n, [&](const U* k, int nv) {
+    uint32_t take = 0u;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const U o = KO::to_ordered(k[e]);
+      if (e < nv && o >= lo && o <= hi) take |= 1u << e;
+      below += (e < nv && o < lo) ? 1u : 0u;
+    }
+    to_cand.add(k, take);
+  });
+  to_cand.flush();
+  below = __reduce_add_sync(0xFFFFFFFFu, below);
+  if ((threadIdx.x & 31) == 0 && below) atomicAdd(&st->below, (unsigned long long)below);
+}
+
+// One thread: select among the candidates when the rank falls among them, else over all keys.
+static __global__ void select_decide_kernel(SelectState* st, int64_t n, int64_t rank) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int64_t c = st->cand_count, b = int64_t(st->below);
+  if (b <= rank && rank < b + c) {
+    st->mode = SEL_MODE_CAND;
+    st->n_total = c;
+    st->rank = rank - b;
+    st->less = b;
+  } else {
+    st->mode = SEL_MODE_FULL;
+    st->n_total = n;
+    st->rank = rank;
+    st->less = 0;
+    st->cand_count = 0;
+  }
 }
 
 // One read of the keys: the keys whose ordered value is at least the threshold go to `cand`.

@@ -20,27 +20,38 @@ inline int select_grid(hpcs_ctx* ctx, int64_t n, int key_bytes) {
 
 // Radix select of the key of 0-based rank `rank` among n keys at device pointer d.  Leaves
 // the SelectState in ctx->aux1 (prefix = the ordered bits of the selected key, less/eq counts).
-// With top_out (top-k of the k = n - rank largest), the level-0 compaction also writes the
-// keys above the level-0 bin to top_out.
+// One read of the keys in the common case: a sampled window around the rank, one read that
+// counts the keys below it and keeps the keys inside (topk.cuh), the radix select over those;
+// the two-read select over all keys when the rank falls outside the window.
 template <class U, int KIND>
-inline int enqueue_select(hpcs_ctx* ctx, const U* d, int64_t n, int64_t rank, cudaStream_t s, SelectState** out,
-                          U* top_out = nullptr) {
+inline int enqueue_select(hpcs_ctx* ctx, const U* d, int64_t n, int64_t rank, cudaStream_t s, SelectState** out) {
   constexpr int BITS = int(sizeof(U) * 8);
   constexpr int LEVELS = BITS / 8;
+  constexpr int S = topk_sample_size<U>();
   int rc;
   if ((rc = ensure(ctx, ctx->aux1, sizeof(SelectState))) != HPCS_OK) return rc;
   if ((rc = ensure(ctx, ctx->aux0, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
   SelectState* st = static_cast<SelectState*>(ctx->aux1.ptr);
   U* cand = static_cast<U*>(ctx->aux0.ptr);
-  KernelTimer kt(ctx, s, HPCS_K_TOPK);
-  select_init_kernel<<<1, 256, 0, s>>>(st, rank, n);
+  // the sample rank of the selected key has standard deviation sqrt(S p (1 - p)), p = rank / n;
+  // the window reaches 6 of them plus 9 samples to each side
+  const double p = n > 0 ? double(rank) / double(n) : 0.0;
+  const int64_t m = int64_t(6.0 * std::sqrt(double(S) * p * (1.0 - p)) + 9.0) + 1;
   const int grid = select_grid(ctx, n, int(sizeof(U)));
-  select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, nullptr, n, st, BITS - 8);
+  const int64_t expect = n < int64_t(4) * S ? n : int64_t(double(2 * m + 1) / S * double(n));
+  const int cgrid = select_grid(ctx, 2 * expect, int(sizeof(U)));
+  KernelTimer kt(ctx, s, HPCS_K_TOPK);
+  select_sample_kernel<U, KIND><<<1, TOPK_SAMPLE_NT, 0, s>>>(d, n, rank, m, st);
+  select_window_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, cand, st);
+  select_decide_kernel<<<1, 32, 0, s>>>(st, n, rank);
+  // level 0: over the candidates, or (fallback) over all keys with the compaction
+  select_hist_kernel<U, KIND><<<cgrid, SEL_NT, 0, s>>>(cand, &st->cand_count, 0, st, BITS - 8, SEL_MODE_CAND);
+  select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, nullptr, n, st, BITS - 8, SEL_MODE_FULL);
   select_pick_kernel<U><<<1, 256, 0, s>>>(st, BITS - 8, LEVELS == 1);
-  select_compact_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, cand, st, top_out, n - rank);
+  select_compact_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(d, n, cand, st, nullptr, 0, SEL_MODE_FULL);
   for (int l = 1; l < LEVELS; l++) {
     const int shift = BITS - 8 * (l + 1);
-    select_hist_kernel<U, KIND><<<grid, SEL_NT, 0, s>>>(cand, &st->cand_count, 0, st, shift);
+    select_hist_kernel<U, KIND><<<cgrid, SEL_NT, 0, s>>>(cand, &st->cand_count, 0, st, shift);
     select_pick_kernel<U><<<1, 256, 0, s>>>(st, shift, l == LEVELS - 1);
   }
   HPCS_CUDA(cudaGetLastError());

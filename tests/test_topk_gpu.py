@@ -66,6 +66,26 @@ def test_select_topk_duplicates(ctx, orc, kind):
         np.testing.assert_array_equal(np.sort(got[k:]), srt[k:])
 
 
+@pytest.mark.parametrize("poison", ["max", "zero"])
+def test_sampled_window_falls_back(ctx, orc, poison):
+    """The select and the k largest read a strided sample (8192 keys at stride n // 8192) to
+    choose the keys worth keeping.  Keys planted at exactly the sample positions make the sample
+    lie about the distribution; the selection must then take its fallback path (all keys, two
+    reads) and still return the exact result."""
+    n = 1_000_003
+    a = datagen.u32_uniform(n, seed=11)
+    stride = n // 8192
+    a[np.arange(8192, dtype=np.int64) * stride] = np.uint32(0xFFFFFFFF if poison == "max" else 0)
+    srt = np.sort(a)
+    for k in (0, 17, n // 2, n - 5):
+        got = a.copy()
+        ctx.select_topk(got, k)
+        assert got[k] == srt[k]
+        np.testing.assert_array_equal(np.sort(got[k:]), srt[k:])
+    for k in (10, 5000, 100_000):
+        np.testing.assert_array_equal(ctx.topk_largest(a, k), srt[n - k:])
+
+
 @pytest.mark.parametrize("k", [0, 1, 10, 1000, 100_000])
 @pytest.mark.parametrize("dt", ["u32", "i32", "f32", "u64"])
 def test_topk_largest(ctx, orc, dt, k):
