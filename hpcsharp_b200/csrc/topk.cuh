@@ -7,20 +7,22 @@
 // movers clobber the prefix; here the prefix is defined too: a[0..k-1] holds the k smallest.
 //
 // Selection: an MSD radix select over the order-transformed key (the same transforms as the
-// sort), 8 bits per level.  Level 0 histograms all n keys; the keys of the chosen bin are
-// compacted into a candidate buffer (about n/256 of them for spread keys) and the remaining
-// levels histogram only candidates that match the prefix chosen so far.  A one-block "pick"
-// kernel after each histogram advances the device-side SelectState, so nothing returns to the
-// host between levels.  The passes over all n keys read them with 16-byte loads, several in
-// flight per thread (visit_keys); compactions stage kept keys per warp in shared memory and
-// take one global atomic per 1 KiB of them.
+// sort), 8 bits per level.  A strided sample of the keys first bounds where the selected key
+// lies (a window around its rank; for the k largest, a threshold), and one read of all keys
+// keeps the keys inside (the candidates) and counts those below.  The levels then histogram
+// only candidates that match the prefix chosen so far.  When the sample misled (the rank falls
+// outside the candidates), the select runs over all keys instead: level 0 histograms all n
+// keys and the keys of the chosen bin are compacted into the candidate buffer.  The choice is
+// made on the device.  A one-block "pick" kernel after each histogram advances the device-side
+// SelectState, so nothing returns to the host between levels.  The passes over all n keys read
+// them with 16-byte loads, several in flight per thread (visit_keys); compactions stage kept
+// keys per warp in shared memory and take one global atomic per 1 KiB of them.
 //
 // Rearrangement: a stable three-way partition (keys < v, == v, > v around the selected key v)
-// in three kernels -- per-tile class counts, a one-block scan, a stable per-tile scatter.
-// The k largest ("top-k" of a serving request) are the keys > v, compacted, plus copies of v
-// up to k, then sorted ascending with the LSD sort so the output bytes are deterministic.
-// Keys above the level-0 bin are all > v: the level-0 compaction writes them to the output
-// at once, and the final gather scans only the candidates.  So top-k reads the n keys twice.
+// -- per-tile class counts, a two-level scan of them, a stable per-tile scatter.
+// The k largest ("top-k" of a serving request) are the keys > v among the candidates plus
+// copies of v up to k, sorted ascending (in one CTA for up to 8 Ki keys, else with the LSD
+// sort) so the output bytes are deterministic.
 #pragma once
 #include <cstdint>
 
