@@ -447,7 +447,15 @@ static __global__ void topk_decide_kernel(SelectState* st, int64_t n, int64_t k)
 }
 
 // ---- stable three-way partition around the selected key -----------------------------
-constexpr int PART_NT = 256, PART_KPT = 16, PART_TILE = PART_NT * PART_KPT;
+// Each warp owns a sub-tile of PART_SUB consecutive keys and partitions it on its own, with no
+// CTA barrier: row j of the sub-tile is keys j * 32 + lane (coalesced loads), a key's stable
+// slot among its class comes from the class ballots of its row and the rows before it, the
+// warp stages the sub-tile in class order in its own shared memory and writes each class's run
+// with consecutive lanes at consecutive positions.  The sub-tiles' class counts (one read) and
+// a two-level scan of them give every sub-tile its output starts.
+constexpr int PART_NT = 256, PART_KPT = 16;
+constexpr int PART_SUB = 32 * PART_KPT;                  // keys per warp sub-tile
+constexpr int PART_SUBS_PER_CTA = PART_NT / 32;
 
 template <class U, int KIND>
 __device__ __forceinline__ int part_class(U k, U v_ordered) {
@@ -457,36 +465,36 @@ __device__ __forceinline__ int part_class(U k, U v_ordered) {
 
 template <class U, int KIND>
 __global__ void __launch_bounds__(PART_NT) partition_count_kernel(const U* __restrict__ keys, int64_t n,
-                                                                  const SelectState* st, uint32_t* tile_counts) {
-  __shared__ uint32_t c[3];
+                                                                  const SelectState* st, uint32_t* sub_counts) {
   const U v = U(st->prefix);
-  if (threadIdx.x < 3) c[threadIdx.x] = 0;
-  __syncthreads();
-  const int64_t base = int64_t(blockIdx.x) * PART_TILE;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t sub = int64_t(blockIdx.x) * PART_SUBS_PER_CTA + warp;
+  const int64_t base = sub * PART_SUB;
+  if (base >= n) return;  // warp-uniform
+  const int sub_n = int(n - base < PART_SUB ? n - base : PART_SUB);
   uint32_t l = 0, e = 0, g = 0;
 #pragma unroll
-  for (int i = threadIdx.x; i < PART_TILE; i += PART_NT) {
-    const int64_t j = base + i;
-    if (j < n) {
-      const int cl = part_class<U, KIND>(keys[j], v);
+  for (int j = 0; j < PART_KPT; j++) {
+    const int i = j * 32 + lane;
+    if (i < sub_n) {
+      const int cl = part_class<U, KIND>(keys[base + i], v);
       l += cl == 0;
       e += cl == 1;
       g += cl == 2;
     }
   }
-  atomicAdd(&c[0], l);
-  atomicAdd(&c[1], e);
-  atomicAdd(&c[2], g);
-  __syncthreads();
-  if (threadIdx.x < 3) tile_counts[int64_t(blockIdx.x) * 3 + threadIdx.x] = c[threadIdx.x];
+  l = __reduce_add_sync(0xFFFFFFFFu, l);
+  e = __reduce_add_sync(0xFFFFFFFFu, e);
+  g = __reduce_add_sync(0xFFFFFFFFu, g);
+  if (lane < 3) sub_counts[sub * 3 + lane] = lane == 0 ? l : (lane == 1 ? e : g);
 }
 
-// Scan of the per-tile class counts in two levels: partition_block_scan_kernel turns the
-// counts of each run of 1024 tiles into starts within the run and records the run's totals;
-// partition_top_scan_kernel (one CTA) turns the run totals into run starts, class c's run
-// starting after all keys of the classes below it (st->less, st->eq).  A tile's start is its
-// run's start plus its start within the run.  (A single CTA stepping through all tiles took
-// 109-143 us for 65,536 tiles.)
+// Scan of the per-sub-tile class counts in two levels: partition_block_scan_kernel turns the
+// counts of each run of PART_SCAN_RUN sub-tiles into starts within the run (a separate array:
+// the scatter reads both) and records the run's totals; partition_top_scan_kernel (one CTA) turns the run totals into run starts, class
+// c's run starting after all keys of the classes below it (st->less, st->eq).  A sub-tile's
+// start is its run's start plus its start within the run.  (A single CTA stepping through all
+// 4096-key tiles took 109-143 us for 65,536 tiles.)
 constexpr int PART_SCAN_RUN = 1024;
 
 template <int NT>
@@ -516,137 +524,111 @@ __device__ __forceinline__ void block_exclusive_scan3(const uint32_t (&v)[3], ui
     excl[c] = before + incl[c] - v[c];
     total[c] = all;
   }
+  __syncthreads();  // wsum may be rewritten by a following call
 }
 
-static __global__ void __launch_bounds__(PART_SCAN_RUN) partition_block_scan_kernel(uint32_t* tile_counts, int64_t tiles,
+static __global__ void __launch_bounds__(PART_SCAN_RUN) partition_block_scan_kernel(const uint32_t* sub_counts,
+                                                                                   int64_t subs, uint32_t* sub_starts,
                                                                                    uint32_t* run_totals) {
   __shared__ uint32_t wsum[3][PART_SCAN_RUN / 32];
   const int64_t t = int64_t(blockIdx.x) * PART_SCAN_RUN + threadIdx.x;
   uint32_t v[3] = {0u, 0u, 0u}, excl[3], total[3];
-  if (t < tiles) {
+  if (t < subs) {
 #pragma unroll
-    for (int c = 0; c < 3; c++) v[c] = tile_counts[t * 3 + c];
+    for (int c = 0; c < 3; c++) v[c] = sub_counts[t * 3 + c];
   }
   block_exclusive_scan3<PART_SCAN_RUN>(v, excl, total, wsum);
-  if (t < tiles) {
+  if (t < subs) {
 #pragma unroll
-    for (int c = 0; c < 3; c++) tile_counts[t * 3 + c] = excl[c];
+    for (int c = 0; c < 3; c++) sub_starts[t * 3 + c] = excl[c];
   }
   if (threadIdx.x < 3) run_totals[int64_t(blockIdx.x) * 3 + threadIdx.x] = total[threadIdx.x];
 }
 
-// runs <= 1024 (n < 2^31 keys in 4096-key tiles is at most 512 runs)
-static __global__ void __launch_bounds__(1024) partition_top_scan_kernel(uint32_t* run_totals, int runs,
+// One CTA over all runs, 1024 at a time with a carry.
+static __global__ void __launch_bounds__(1024) partition_top_scan_kernel(uint32_t* run_totals, int64_t runs,
                                                                          const SelectState* st) {
   __shared__ uint32_t wsum[3][32];
-  const int r = threadIdx.x;
-  uint32_t v[3] = {0u, 0u, 0u}, excl[3], total[3];
-  if (r < runs) {
-#pragma unroll
-    for (int c = 0; c < 3; c++) v[c] = run_totals[r * 3 + c];
-  }
-  block_exclusive_scan3<1024>(v, excl, total, wsum);
   const uint32_t less = uint32_t(st->less), eq = uint32_t(st->eq);
-  if (r < runs) {
-    run_totals[r * 3 + 0] = excl[0];
-    run_totals[r * 3 + 1] = less + excl[1];
-    run_totals[r * 3 + 2] = less + eq + excl[2];
+  uint32_t carry[3] = {0u, less, less + eq};
+  for (int64_t r0 = 0; r0 < runs; r0 += 1024) {
+    const int64_t r = r0 + threadIdx.x;
+    uint32_t v[3] = {0u, 0u, 0u}, excl[3], total[3];
+    if (r < runs) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) v[c] = run_totals[r * 3 + c];
+    }
+    block_exclusive_scan3<1024>(v, excl, total, wsum);
+    if (r < runs) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) run_totals[r * 3 + c] = carry[c] + excl[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) carry[c] += total[c];
   }
 }
 
-// Each thread takes PART_KPT consecutive keys (blocked: 16-byte loads when the keys are
-// aligned), so a block scan of the per-thread class counts gives stable positions.  The tile is
-// staged in shared memory in class order and written by consecutive threads to consecutive
-// positions of each class's run.
 template <class U, int KIND>
 __global__ void __launch_bounds__(PART_NT) partition_scatter_kernel(const U* __restrict__ keys, int64_t n,
                                                                     const SelectState* st,
-                                                                    const uint32_t* tile_starts,
+                                                                    const uint32_t* sub_counts,
+                                                                    const uint32_t* sub_starts,
                                                                     const uint32_t* run_starts,
                                                                     U* __restrict__ out) {
-  constexpr int E = int(16 / sizeof(U));
-  static_assert(PART_KPT % E == 0, "whole vectors per thread");
-  __shared__ uint32_t wsum[3][PART_NT / 32];
-  __shared__ uint32_t s_at[3];  // start of each class's run in the staged tile
-  // staged slot j lives at j + j/32: lanes writing about PART_KPT/2 slots apart land in
-  // different banks
-  __shared__ U s_k[PART_TILE + PART_TILE / 32];
+  // staged slot j lives at j + j/32 of the warp's buffer
+  __shared__ U s_k[PART_SUBS_PER_CTA][PART_SUB + PART_SUB / 32];
   const U v = U(st->prefix);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int64_t tile0 = int64_t(blockIdx.x) * PART_TILE;
-  const int64_t base = tile0 + int64_t(tid) * PART_KPT;
-  const int tile_n = int(n - tile0 < PART_TILE ? n - tile0 : PART_TILE);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t sub = int64_t(blockIdx.x) * PART_SUBS_PER_CTA + warp;
+  const int64_t base = sub * PART_SUB;
+  if (base >= n) return;  // warp-uniform; nothing below waits on other warps
+  const int sub_n = int(n - base < PART_SUB ? n - base : PART_SUB);
+  const U* kin = keys + base;
   U k[PART_KPT];
-  uint8_t cls[PART_KPT];
-  uint32_t cnt[3] = {0, 0, 0};
-  const bool vec = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0 && base + PART_KPT <= n;
-  if (vec) {
-    union {
-      uint4 v;
-      U k[E];
-    } u;
+  uint32_t cls[PART_KPT];
+  if (sub_n == PART_SUB) {  // warp-uniform: full sub-tiles need no bounds
 #pragma unroll
-    for (int q = 0; q < PART_KPT / E; q++) {
-      u.v = __ldg(reinterpret_cast<const uint4*>(keys + base) + q);
-#pragma unroll
-      for (int e = 0; e < E; e++) k[q * E + e] = u.k[e];
+    for (int j = 0; j < PART_KPT; j++) {
+      k[j] = kin[j * 32 + lane];
+      cls[j] = uint32_t(part_class<U, KIND>(k[j], v));
     }
   } else {
 #pragma unroll
-    for (int i = 0; i < PART_KPT; i++) k[i] = base + i < n ? keys[base + i] : U(0);
-  }
-#pragma unroll
-  for (int i = 0; i < PART_KPT; i++) {
-    cls[i] = 3;
-    if (base + i < n) {
-      cls[i] = uint8_t(part_class<U, KIND>(k[i], v));
-      cnt[cls[i]]++;
+    for (int j = 0; j < PART_KPT; j++) {
+      const int i = j * 32 + lane;
+      k[j] = i < sub_n ? kin[i] : U(0);
+      cls[j] = i < sub_n ? uint32_t(part_class<U, KIND>(k[j], v)) : 3u;
     }
   }
-  uint32_t excl[3];
+  // the class runs of the staged sub-tile start at its class counts' prefix sums
+  const uint32_t* sc = sub_counts + sub * 3;
+  const uint32_t at1 = sc[0], at2 = sc[0] + sc[1];
+  U* sw = s_k[warp];
+  const uint32_t lt = lanemask_lt();
+  uint32_t r0 = 0, r1 = at1, r2 = at2;  // next staged slot per class (uniform over the warp)
 #pragma unroll
-  for (int c = 0; c < 3; c++) {
-    uint32_t incl = cnt[c];
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if (lane >= o) incl += y;
-    }
-    excl[c] = incl - cnt[c];
-    if (lane == 31) wsum[c][warp] = incl;
+  for (int j = 0; j < PART_KPT; j++) {
+    const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, cls[j] == 0u);
+    const uint32_t m1 = __ballot_sync(0xFFFFFFFFu, cls[j] == 1u);
+    const uint32_t m2 = __ballot_sync(0xFFFFFFFFu, cls[j] == 2u);
+    const uint32_t mine = cls[j] == 0u ? m0 : (cls[j] == 1u ? m1 : m2);
+    const uint32_t run = cls[j] == 0u ? r0 : (cls[j] == 1u ? r1 : r2);
+    const uint32_t slot = run + __popc(mine & lt);
+    if (cls[j] < 3u) sw[slot + (slot >> 5)] = k[j];
+    r0 += __popc(m0);
+    r1 += __popc(m1);
+    r2 += __popc(m2);
   }
-  __syncthreads();
-  if (tid == 0) {
-    uint32_t at = 0;
-    for (int c = 0; c < 3; c++) {
-      s_at[c] = at;
-      for (int w = 0; w < PART_NT / 32; w++) at += wsum[c][w];
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    uint32_t wb = 0;
-    for (int w = 0; w < warp; w++) wb += wsum[c][w];
-    excl[c] += wb + s_at[c];
-  }
-  uint32_t e0 = excl[0], e1 = excl[1], e2 = excl[2];  // next slot per class (no dynamic index)
-#pragma unroll
-  for (int i = 0; i < PART_KPT; i++) {
-    if (cls[i] < 3) {
-      const uint32_t j = cls[i] == 0 ? e0++ : (cls[i] == 1 ? e1++ : e2++);
-      s_k[j + (j >> 5)] = k[i];
-    }
-  }
-  __syncthreads();
-  const uint32_t at1 = s_at[1], at2 = s_at[2];
-  const uint32_t* ts = tile_starts + int64_t(blockIdx.x) * 3;
-  const uint32_t* rs = run_starts + int64_t(blockIdx.x / PART_SCAN_RUN) * 3;
-  const int64_t o0 = int64_t(rs[0]) + ts[0], o1 = int64_t(rs[1]) + ts[1] - at1, o2 = int64_t(rs[2]) + ts[2] - at2;
-  for (int j = tid; j < tile_n; j += PART_NT) {
+  __syncwarp();
+  // output positions fit 32 bits (n < 2^31)
+  const uint32_t* ss = sub_starts + sub * 3;
+  const uint32_t* rs = run_starts + (sub / PART_SCAN_RUN) * 3;
+  const uint32_t o0 = rs[0] + ss[0], o1 = rs[1] + ss[1] - at1, o2 = rs[2] + ss[2] - at2;
+  const uint32_t n32 = uint32_t(n);
+  for (int j = lane; j < sub_n; j += 32) {
     const uint32_t uj = uint32_t(j);
-    const int64_t pos = (uj < at1 ? o0 : (uj < at2 ? o1 : o2)) + j;
-    if (pos < n) out[pos] = s_k[j + (j >> 5)];
+    const uint32_t pos = (uj < at1 ? o0 : (uj < at2 ? o1 : o2)) + uj;
+    if (pos < n32) out[pos] = sw[j + (j >> 5)];
   }
 }
 

@@ -62,18 +62,19 @@ inline int enqueue_select(hpcs_ctx* ctx, const U* d, int64_t n, int64_t rank, cu
 // Stable three-way partition of d[0..n) around the selected key into out.
 template <class U, int KIND>
 inline int enqueue_partition(hpcs_ctx* ctx, const U* d, int64_t n, SelectState* st, U* out, cudaStream_t s) {
-  const int64_t tiles = (n + PART_TILE - 1) / PART_TILE;
-  const int64_t runs = (tiles + PART_SCAN_RUN - 1) / PART_SCAN_RUN;
-  if (runs > 1024) return fail(HPCS_ERR_RANGE, "partition of more than 2^32 keys");
+  const int64_t subs = (n + PART_SUB - 1) / PART_SUB;
+  const int64_t runs = (subs + PART_SCAN_RUN - 1) / PART_SCAN_RUN;
+  const int64_t ctas = (subs + PART_SUBS_PER_CTA - 1) / PART_SUBS_PER_CTA;
   int rc;
-  if ((rc = ensure(ctx, ctx->aux2, size_t(tiles + runs) * 3 * 4)) != HPCS_OK) return rc;
-  uint32_t* tc = static_cast<uint32_t*>(ctx->aux2.ptr);
-  uint32_t* rt = tc + tiles * 3;
+  if ((rc = ensure(ctx, ctx->aux2, size_t(2 * subs + runs) * 3 * 4)) != HPCS_OK) return rc;
+  uint32_t* sc = static_cast<uint32_t*>(ctx->aux2.ptr);  // per sub-tile: class counts
+  uint32_t* ss = sc + subs * 3;                          // class starts within the run
+  uint32_t* rt = ss + subs * 3;                          // per run: totals, then starts
   KernelTimer kt(ctx, s, HPCS_K_TOPK);
-  partition_count_kernel<U, KIND><<<int(tiles), PART_NT, 0, s>>>(d, n, st, tc);
-  partition_block_scan_kernel<<<int(runs), PART_SCAN_RUN, 0, s>>>(tc, tiles, rt);
-  partition_top_scan_kernel<<<1, 1024, 0, s>>>(rt, int(runs), st);
-  partition_scatter_kernel<U, KIND><<<int(tiles), PART_NT, 0, s>>>(d, n, st, tc, rt, out);
+  partition_count_kernel<U, KIND><<<int(ctas), PART_NT, 0, s>>>(d, n, st, sc);
+  partition_block_scan_kernel<<<int(runs), PART_SCAN_RUN, 0, s>>>(sc, subs, ss, rt);
+  partition_top_scan_kernel<<<1, 1024, 0, s>>>(rt, runs, st);
+  partition_scatter_kernel<U, KIND><<<int(ctas), PART_NT, 0, s>>>(d, n, st, sc, ss, rt, out);
   HPCS_CUDA(cudaGetLastError());
   return HPCS_OK;
 }
