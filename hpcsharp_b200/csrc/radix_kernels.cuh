@@ -123,6 +123,12 @@ struct HistSmem {
   static constexpr size_t BYTES = size_t(P) * RADIX * COPIES * 4;
 };
 
+// 16-byte vectors in flight per thread in the histogram's read (8 x 16 B x 1024 threads = 128 KiB
+// per SM).
+#ifndef HIST_VIF
+#define HIST_VIF 8
+#endif
+
 // cta / ncta: this CTA's index and the CTA count of this array's histogram (the grid of a
 // single-array launch; the array's ranges in the batched sort's grid-level launch).
 template <class U, int KIND, int NT>
@@ -165,13 +171,13 @@ __device__ __forceinline__ void hist_all_digits_body(const U* __restrict__ keys,
     stride = NT;
     owns_tail = hi == n;
   }
-  // 4 vectors in flight per thread per iteration
-  for (; i + 3 * stride < vend; i += 4 * stride) {
-    uint4 v[4];
+  // HIST_VIF vectors in flight per thread per iteration
+  for (; i + (HIST_VIF - 1) * stride < vend; i += HIST_VIF * stride) {
+    uint4 v[HIST_VIF];
 #pragma unroll
-    for (int u = 0; u < 4; u++) v[u] = ldg_stream_v4(vkeys + i + u * stride);
+    for (int u = 0; u < HIST_VIF; u++) v[u] = ldg_stream_v4(vkeys + i + u * stride);
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
+    for (int u = 0; u < HIST_VIF; u++) {
       const U* e = reinterpret_cast<const U*>(&v[u]);
 #pragma unroll
       for (int j = 0; j < VEC; j++) count_key(e[j]);
