@@ -102,6 +102,11 @@ extern "C" int hpcs_sort_u32_dev_noalloc(uint32_t* keys, int64_t n, void* stream
   int rc = na_setup(dev, &d);
   if (rc != HPCS_OK) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the call waits for its stream and reads the error word back: it cannot be captured
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  HPCS_CUDA(cudaStreamIsCapturing(s, &cap));
+  if (cap != cudaStreamCaptureStatusNone)
+    return fail(HPCS_ERR_UNSUPPORTED, "the no-allocation sort cannot be called while its stream is being captured");
   const int64_t units = (n + NA_TILE - 1) / NA_TILE;
 
   SortArgs args{};

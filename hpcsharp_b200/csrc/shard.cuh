@@ -60,14 +60,17 @@ __device__ __forceinline__ void shard_load_splitters(ShardSplit<U>& sp, const U*
 // Number of splitters at or below (ok, g): the part of an element with ordered key ok.  A
 // branchless search over 2^LOG - 1 keys counts the splitters whose key is below ok; the
 // splitters whose key equals ok follow in ascending position, and the (rarely entered) loop
-// counts those at or below g.  m = parts - 1 <= 2^LOG - 1.
+// counts those at or below g = gbase + i (formed only there).  m = parts - 1 <= 2^LOG - 1.
 template <class U, int LOG>
-__device__ __forceinline__ int shard_part_of(const ShardSplit<U>& sp, int m, U ok, int64_t g) {
+__device__ __forceinline__ int shard_part_of(const ShardSplit<U>& sp, int m, U ok, int64_t gbase, int i) {
   int pos = 0;
 #pragma unroll
   for (int l = LOG - 1; l >= 0; l--)
     if (sp.key[pos + (1 << l) - 1] < ok) pos += 1 << l;
-  while (pos < m && sp.key[pos] == ok && sp.gpos[pos] <= g) pos++;
+  if (pos < m && sp.key[pos] == ok) {
+    const int64_t g = gbase + i;
+    while (pos < m && sp.key[pos] == ok && sp.gpos[pos] <= g) pos++;
+  }
   return pos;
 }
 
@@ -133,7 +136,7 @@ __global__ void __launch_bounds__(SHARD_COUNT_NT, 4) shard_count_kernel(const U*
     for (int r = 0; r < SHARD_KPT; r++) {
       const int i = t + r * NT + tid;
       const bool valid = full || i < len;
-      const int b = valid ? shard_part_of<U, LOG>(sp, parts - 1, KeyOrder<U, KIND>::to_ordered(k[r]), gbase + i)
+      const int b = valid ? shard_part_of<U, LOG>(sp, parts - 1, KeyOrder<U, KIND>::to_ordered(k[r]), gbase, i)
                           : parts;
       if (PACKED) {
         const uint32_t inc = valid ? 1u << (8 * (b & 3)) : 0u;
@@ -224,7 +227,7 @@ __global__ void __launch_bounds__(SHARD_NT, (shard_ctas_per_sm<U, ITEMS>())) sha
   __shared__ int64_t s_tile[SHARD_MAX_PARTS];  // global base of each part's run in this tile
   __shared__ uint32_t s_len[SHARD_MAX_PARTS];  // length of each part's run in this tile
   __shared__ uint32_t s_at[SHARD_MAX_PARTS];   // start of each part's run in the staged tile
-  __shared__ int64_t s_out[SHARD_MAX_PARTS];   // s_tile - s_at: output index of staged slot 0
+  __shared__ uint32_t s_out[SHARD_MAX_PARTS];  // s_tile - s_at (mod 2^32): output index of staged slot 0
   extern __shared__ __align__(16) unsigned char s_raw[];
   U* stage_k = reinterpret_cast<U*>(s_raw);
   uint32_t* s_cnt = reinterpret_cast<uint32_t*>(s_raw + size_t(SHARD_TILE) * sizeof(U));  // [SHARD_SUB][parts]
@@ -259,17 +262,26 @@ __global__ void __launch_bounds__(SHARD_NT, (shard_ctas_per_sm<U, ITEMS>())) sha
     uint32_t vn[SHARD_KPT];
     int b[SHARD_KPT];
     int rk[SHARD_KPT];
+    if (t + 2 * SHARD_TILE <= len) {  // the next tile is whole (uniform over the CTA)
 #pragma unroll
-    for (int r = 0; r < SHARD_KPT; r++) {
-      const int i = t + SHARD_TILE + r * SHARD_NT + tid;
-      kn[r] = i < len ? kr[i] : U(0);
-      if (ITEMS) vn[r] = i < len ? vr[i] : 0u;
+      for (int r = 0; r < SHARD_KPT; r++) {
+        const int i = t + SHARD_TILE + r * SHARD_NT + tid;
+        kn[r] = kr[i];
+        if (ITEMS) vn[r] = vr[i];
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < SHARD_KPT; r++) {
+        const int i = t + SHARD_TILE + r * SHARD_NT + tid;
+        kn[r] = i < len ? kr[i] : U(0);
+        if (ITEMS) vn[r] = i < len ? vr[i] : 0u;
+      }
     }
     if (full) {  // every key of the tile is in range: LOG ballots
 #pragma unroll
       for (int r = 0; r < SHARD_KPT; r++) {
         const int i = t + r * SHARD_NT + tid;
-        b[r] = shard_part_of<U, LOG>(sp, parts - 1, KeyOrder<U, KIND>::to_ordered(k[r]), gbase + i);
+        b[r] = shard_part_of<U, LOG>(sp, parts - 1, KeyOrder<U, KIND>::to_ordered(k[r]), gbase, i);
         const uint32_t peers = shard_peers<LOG>(b[r]);
         rk[r] = __popc(peers & lanemask_lt());
         if (rk[r] == 0) s_cnt[(r * SHARD_NW + warp) * parts + b[r]] = __popc(peers);
@@ -278,7 +290,7 @@ __global__ void __launch_bounds__(SHARD_NT, (shard_ctas_per_sm<U, ITEMS>())) sha
 #pragma unroll
       for (int r = 0; r < SHARD_KPT; r++) {
         const int i = t + r * SHARD_NT + tid;
-        b[r] = i < len ? shard_part_of<U, LOG>(sp, parts - 1, KeyOrder<U, KIND>::to_ordered(k[r]), gbase + i)
+        b[r] = i < len ? shard_part_of<U, LOG>(sp, parts - 1, KeyOrder<U, KIND>::to_ordered(k[r]), gbase, i)
                        : parts;
         const uint32_t peers = shard_peers<LOG + 1>(b[r]);
         rk[r] = __popc(peers & lanemask_lt());
@@ -332,11 +344,11 @@ __global__ void __launch_bounds__(SHARD_NT, (shard_ctas_per_sm<U, ITEMS>())) sha
       const uint32_t first_half = __shfl_sync(0xFFFFFFFFu, ia, 31);
       if (lane < parts) {
         s_at[lane] = ia - a;
-        s_out[lane] = s_tile[lane] - int64_t(ia - a);
+        s_out[lane] = uint32_t(s_tile[lane]) - (ia - a);
       }
       if (lane + 32 < parts) {
         s_at[lane + 32] = first_half + ic - c;
-        s_out[lane + 32] = s_tile[lane + 32] - int64_t(first_half + ic - c);
+        s_out[lane + 32] = uint32_t(s_tile[lane + 32]) - (first_half + ic - c);
       }
     }
     __syncthreads();
@@ -352,7 +364,7 @@ __global__ void __launch_bounds__(SHARD_NT, (shard_ctas_per_sm<U, ITEMS>())) sha
     __syncthreads();
     const int cnt = len - t < SHARD_TILE ? len - t : SHARD_TILE;
     for (int j = tid; j < cnt; j += SHARD_NT) {
-      const int64_t pos = s_out[stage_p[j]] + j;
+      const uint32_t pos = s_out[stage_p[j]] + uint32_t(j);  // shards hold fewer than 2^31 keys
       keys_out[pos] = stage_k[j];
       if (ITEMS) items_out[pos] = stage_v[j];
     }

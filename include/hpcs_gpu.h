@@ -399,10 +399,11 @@ int hpcs_server_destroy(hpcs_server* server);
  * no cudaMalloc, cudaFree or other allocating routine is called.
  *   - Larger n returns HPCS_ERR_RANGE; an unaligned pointer HPCS_ERR_UNSUPPORTED.
  *   - Runs on `stream` (a cudaStream_t of the current device) and returns when the sort has
- *     finished, reporting a device-side wait that ran out as HPCS_ERR_DEVICE_TIMEOUT.
+ *     finished, reporting a device-side wait that ran out as HPCS_ERR_DEVICE_TIMEOUT.  It
+ *     synchronises with the stream, so it cannot be part of a CUDA graph: a call on a stream
+ *     that is being captured returns HPCS_ERR_UNSUPPORTED and enqueues nothing.
  *   - The first call on a device also does a one-time set-up on the current device (it
- *     looks up the scratch array's device address and sets kernel attributes); make that
- *     first call before any stream capture.
+ *     looks up the scratch array's device address and sets kernel attributes).
  *   - All calls on a device share the one scratch array, which keeps the last call's
  *     contents (each call clears what must start at zero).  Calls that overlap on the GPU --
  *     from several streams or host threads at once -- race and corrupt each other.

@@ -76,3 +76,27 @@ def test_no_alloc_sort_rejects_too_many_keys():
     assert rc == native.HPCS_ERR_RANGE
     assert b"HPCS_NOALLOC_MAX_KEYS" in lib.hpcs_last_error_message()
     assert fn(None, 10, None) == native.HPCS_ERR_NULL
+
+
+def test_no_alloc_sort_refuses_a_stream_under_capture():
+    """The call synchronises with its stream, so on a stream being captured into a CUDA graph it
+    returns HPCS_ERR_UNSUPPORTED and enqueues nothing (the capture stays valid)."""
+    import torch
+
+    lib, fn = _entry()
+    a = datagen.u32_uniform(10_000, seed=9)
+    t = to_dev(a)
+    s = torch.cuda.Stream()
+    assert fn(t.data_ptr(), a.size, s.cuda_stream) == native.HPCS_OK  # set-up outside any capture
+    torch.cuda.synchronize()
+    u = to_dev(a)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        rc = fn(u.data_ptr(), a.size, s.cuda_stream)
+        u.add_(0)  # the capture holds at least this kernel
+    assert rc == native.HPCS_ERR_UNSUPPORTED
+    assert b"captured" in lib.hpcs_last_error_message()
+    g.replay()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(from_dev(u, np.uint32), a)  # nothing was sorted
+    np.testing.assert_array_equal(from_dev(t, np.uint32), np.sort(a))
