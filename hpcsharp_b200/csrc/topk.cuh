@@ -220,6 +220,13 @@ template <class U>
 __host__ __device__ constexpr int topk_sample_size() {
   return 8192;  // 8 keys per thread in registers
 }
+// The select's window: its width shrinks as 1/sqrt(samples), and at the median it holds a few
+// percent of the keys, so 32-bit keys take four times the samples (32 keys per thread; 64-bit
+// keys stay at 8 per thread, where 16 would spill registers).
+template <class U>
+__host__ __device__ constexpr int select_sample_size() {
+  return sizeof(U) == 4 ? 32768 : 8192;
+}
 constexpr int TOPK_SAMPLE_NT = 1024;
 
 // The ordered value of 0-based ascending rank `rank` among the TOPK_SAMPLE_NT x PER samples o[]
@@ -322,7 +329,7 @@ template <class U, int KIND>
 __global__ void __launch_bounds__(TOPK_SAMPLE_NT) select_sample_kernel(const U* __restrict__ keys, int64_t n,
                                                                        int64_t rank, int64_t m, SelectState* st) {
   using KO = KeyOrder<U, KIND>;
-  constexpr int S = topk_sample_size<U>();
+  constexpr int S = select_sample_size<U>();
   constexpr int PER = S / TOPK_SAMPLE_NT;
   __shared__ uint32_t hist[256];
   __shared__ uint32_t s_wsum[8];

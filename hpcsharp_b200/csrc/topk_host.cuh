@@ -27,7 +27,7 @@ template <class U, int KIND>
 inline int enqueue_select(hpcs_ctx* ctx, const U* d, int64_t n, int64_t rank, cudaStream_t s, SelectState** out) {
   constexpr int BITS = int(sizeof(U) * 8);
   constexpr int LEVELS = BITS / 8;
-  constexpr int S = topk_sample_size<U>();
+  constexpr int S = select_sample_size<U>();
   int rc;
   if ((rc = ensure(ctx, ctx->aux1, sizeof(SelectState))) != HPCS_OK) return rc;
   if ((rc = ensure(ctx, ctx->aux0, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
