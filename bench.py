@@ -207,6 +207,15 @@ def cpu_baseline(dtype: str, n: int, budget_s: float = 15.0):
                       f"quanta), scratch allocated once outside the timed calls, best of 3"}
 
 
+def plain_config(n: int, dtype: str, world: int, digest: str) -> dict:
+    """The plain-sort workload's config, the same dict in both arms (ours and the reference)."""
+    w = 4 if dtype in ("u32", "i32", "f32") else 8
+    return {"workload": f"plain LSD radix sort of {n} {dtype} keys uniform over the key range, stable, "
+                        f"8-bit digits",
+            "n": n, "parallelism": f"replicas x{world}", "input_sha256": digest,
+            "l2": f"inputs {'larger' if n * w > 126 * 2**20 else 'smaller'} than L2 ({n * w} bytes per copy)"}
+
+
 def input_digest(a: np.ndarray) -> str:
     """SHA-256 of the keys a step sorts: both arms print it, so their inputs can be compared."""
     import hashlib
@@ -252,10 +261,8 @@ def run_reference(args, rank: int, world: int):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tot / args.steps * 1e3, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.dtype,
         "data": "synthetic (seeded PCG32 uniform keys)",
-        "config": {"workload": f"plain LSD radix sort of {n} u32 keys uniform over the key range, host-resident, "
-                               "stable, 8-bit digits",
-                   "n": n, "input_sha256": digest,
-                   "l2": f"inputs {'larger' if n * 4 > 126 * 2**20 else 'smaller'} than L2 ({n * 4} bytes)"},
+        "config": plain_config(n, "u32", world, digest),
+        "residency": "host memory (the reference sorts managed host arrays)",
         "cpu_baseline": {"value": round(rate, 4), "unit": UNIT, "cores": th, "kind": "port",
                          "sample": f"the full {n}-key configuration every step; C++ restatement of "
                                    f"SortRadixPar (RadixSortLsdParallel.cs:145-232), 64 Ki work quanta, "
@@ -402,10 +409,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "warmup": args.warmup, "ms_per_step": round(ms_per_step, 5), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": dtype,
             "data": "synthetic (seeded PCG32 uniform keys)",
-            "config": {"workload": f"plain LSD radix sort of {n} {dtype} keys uniform over the key range, "
-                                   f"device-resident, stable, 8-bit digits",
-                       "n": n, "parallelism": f"replicas x{world}", "input_sha256": input_digest(host),
-                       "l2": "inputs larger than L2 (1 GiB per copy); input restored between steps"},
+            "config": plain_config(n, dtype, world, input_digest(host)),
+            "residency": "device memory (value); host memory through the C ABI (e2e, e2e_pinned); "
+                         "inputs restored between steps",
             "roofline": roof, "sort_roofline": sort_roof, "cpu_baseline": cpu, "e2e": e2e, "e2e_pinned": e2e_pinned,
             "gpu_launches": launches, "clocks": clk, "rank_mode": ctx.rank_mode,
         }
