@@ -125,8 +125,8 @@ struct HistSmem {
 
 // 16-byte vectors in flight per thread in the histogram's read (8 x 16 B x 1024 threads = 128 KiB
 // per SM).
-#ifndef HIST_VIF
-#define HIST_VIF 8
+#ifndef HPCS_HIST_VIF
+#define HPCS_HIST_VIF 8
 #endif
 
 // cta / ncta: this CTA's index and the CTA count of this array's histogram (the grid of a
@@ -171,13 +171,13 @@ __device__ __forceinline__ void hist_all_digits_body(const U* __restrict__ keys,
     stride = NT;
     owns_tail = hi == n;
   }
-  // HIST_VIF vectors in flight per thread per iteration
-  for (; i + (HIST_VIF - 1) * stride < vend; i += HIST_VIF * stride) {
-    uint4 v[HIST_VIF];
+  // HPCS_HIST_VIF vectors in flight per thread per iteration
+  for (; i + (HPCS_HIST_VIF - 1) * stride < vend; i += HPCS_HIST_VIF * stride) {
+    uint4 v[HPCS_HIST_VIF];
 #pragma unroll
-    for (int u = 0; u < HIST_VIF; u++) v[u] = ldg_stream_v4(vkeys + i + u * stride);
+    for (int u = 0; u < HPCS_HIST_VIF; u++) v[u] = ldg_stream_v4(vkeys + i + u * stride);
 #pragma unroll
-    for (int u = 0; u < HIST_VIF; u++) {
+    for (int u = 0; u < HPCS_HIST_VIF; u++) {
       const U* e = reinterpret_cast<const U*>(&v[u]);
 #pragma unroll
       for (int j = 0; j < VEC; j++) count_key(e[j]);
