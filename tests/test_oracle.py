@@ -20,6 +20,23 @@ def test_known_answer_program_cs(orc):
         assert b.tolist() == [3, 5, 16, 21, 43, 54]
 
 
+# HPCsharpExamples/HPCsharpExamples/SortOfUserDefinedClass.cs:87-104: userArray.SortRadix(element
+# => element.Key), commented "(stable)", on (Key, Index) = (16,0) (12,1) (18,2) (18,3) (10,4) (2,5);
+# the stable order it prints is (2:5) (10:4) (12:1) (16:0) (18:2) (18:3).
+UDT_EXAMPLE = [(16, 0), (12, 1), (18, 2), (18, 3), (10, 4), (2, 5)]
+UDT_EXAMPLE_SORTED = [(2, 5), (10, 4), (12, 1), (16, 0), (18, 2), (18, 3)]
+
+
+def test_known_answer_user_defined_class_sort(orc):
+    """The key + index pairs sort (the reference's SortRadix by key, RadixSortLsd.cs:1183-1237)
+    on the example's keys, with the index as the item: stable, so the two 18s keep their order."""
+    for kdt in (np.uint32, np.uint64):
+        keys = np.array([k for k, _ in UDT_EXAMPLE], dtype=kdt)
+        items = np.array([i for _, i in UDT_EXAMPLE], dtype=np.uint32)
+        orc.sort_pairs(keys, items)
+        assert list(zip(keys.tolist(), items.tolist())) == UDT_EXAMPLE_SORTED
+
+
 @pytest.mark.parametrize("n", SIZES)
 @pytest.mark.parametrize("dt", ["u32", "i32", "u64", "i64"])
 def test_integer_lsd_matches_std_sort(orc, dt, n):

@@ -241,6 +241,15 @@ def test_peer_mask_ranking_parity(orc, dt):
         c.close()
 
 
+def test_known_answer_user_defined_class_sort():
+    """HPCsharpExamples/HPCsharpExamples/SortOfUserDefinedClass.cs:87-104: SortRadix(element =>
+    element.Key) of the example's (Key, Index) objects, stable: the two 18s keep their order."""
+    items = [(16, 0), (12, 1), (18, 2), (18, 3), (10, 4), (2, 5)]
+    want = [(2, 5), (10, 4), (12, 1), (16, 0), (18, 2), (18, 3)]
+    assert algorithm.SortRadixLsd(items, lambda t: t[0]) == want
+    assert algorithm.SortRadixFaster(items, lambda t: t[0]) == want
+
+
 @pytest.mark.parametrize("wide", [False, True])
 def test_user_defined_type_sort_by_key(wide):
     """SortRadixLsd(items, getKey) / SortRadixFaster: stable ascending by the extracted key, a
