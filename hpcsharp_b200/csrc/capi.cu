@@ -206,6 +206,19 @@ int probe_shipping_kernels(hpcs_ctx* ctx, int* ok) {
       }
     }
   }
+  // the one-launch sort of small arrays (small_sort.cuh), taken by the default scheme
+  ctx->cfg.pass_scheme = HPCS_PASSES_AUTO;
+  constexpr int64_t n_small = 100003;
+  for (uint32_t values : {20u, 3u}) {
+    if (rc != HPCS_OK) break;
+    probe_fill_kernel<<<ctx->sms * 4, 256, 0, s>>>(keys, nullptr, n_small, values);
+    if ((e = cudaGetLastError()) != cudaSuccess) rc = cuda_fail(e, "probe fill");
+    if (rc == HPCS_OK) rc = enqueue_sort<uint32_t, KIND_UNSIGNED, NoValue>(ctx, keys, nullptr, n_small, s);
+    if (rc == HPCS_OK) {
+      probe_check_kernel<<<ctx->sms * 4, 256, 0, s>>>(keys, nullptr, n_small, bad);
+      if ((e = cudaGetLastError()) != cudaSuccess) rc = cuda_fail(e, "probe check");
+    }
+  }
   ctx->rank_mode = saved_mode;
   ctx->cfg.pass_scheme = saved_scheme;
   uint32_t h = 1;
