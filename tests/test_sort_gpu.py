@@ -314,3 +314,26 @@ def test_counting_sort_device_unaligned(ctx):
     torch.cuda.synchronize()
     ctx.synchronize()
     assert np.array_equal(big[3:].cpu().numpy().view(np.uint16), np.sort(a))
+
+
+SMALL_SORT_SIZES = [4096 * 31 + 1, 131_072, 131_073]  # 32 CTAs (one partial), the maximum, one past it
+
+
+@pytest.mark.parametrize("rank_mode", [0, 1], ids=["ordered_atomic", "peer_mask"])
+@pytest.mark.parametrize("n", SMALL_SORT_SIZES)
+@pytest.mark.parametrize("dt", ["u32", "f32", "i64"])
+def test_small_sort_limits(orc, dt, n, rank_mode):
+    """Keys-only sorts of up to 128 Ki keys run all their passes in one cooperative launch
+    (one 4096-key slice per CTA, a grid barrier between the count and the scatter of each pass);
+    one key more takes the large-array kernels.  Both sides of the limit, both ranking modes,
+    bit-exact against the oracle, with duplicates so that stability across slices matters."""
+    a = datagen.by_name(dt, n, seed=77 + n)
+    a[::3] = a[0]  # a run of equal keys spread over every slice
+    want = oracle_sorted(orc, a)
+    c = native.Context(0, rank_mode=rank_mode)
+    try:
+        got = a.copy()
+        c.sort(got)
+        assert_same_bits(got, want)
+    finally:
+        c.close()
