@@ -210,13 +210,17 @@ int probe_shipping_kernels(hpcs_ctx* ctx, int* ok) {
   ctx->cfg.pass_scheme = HPCS_PASSES_AUTO;
   constexpr int64_t n_small = 100003;
   for (uint32_t values : {20u, 3u}) {
-    if (rc != HPCS_OK) break;
-    probe_fill_kernel<<<ctx->sms * 4, 256, 0, s>>>(keys, nullptr, n_small, values);
-    if ((e = cudaGetLastError()) != cudaSuccess) rc = cuda_fail(e, "probe fill");
-    if (rc == HPCS_OK) rc = enqueue_sort<uint32_t, KIND_UNSIGNED, NoValue>(ctx, keys, nullptr, n_small, s);
-    if (rc == HPCS_OK) {
-      probe_check_kernel<<<ctx->sms * 4, 256, 0, s>>>(keys, nullptr, n_small, bad);
-      if ((e = cudaGetLastError()) != cudaSuccess) rc = cuda_fail(e, "probe check");
+    for (int with_items = 0; with_items < 2 && rc == HPCS_OK; with_items++) {
+      uint32_t* it = with_items ? items : nullptr;
+      probe_fill_kernel<<<ctx->sms * 4, 256, 0, s>>>(keys, it, n_small, values);
+      if ((e = cudaGetLastError()) != cudaSuccess) rc = cuda_fail(e, "probe fill");
+      if (rc == HPCS_OK)
+        rc = with_items ? enqueue_sort<uint32_t, KIND_UNSIGNED, uint32_t>(ctx, keys, items, n_small, s)
+                        : enqueue_sort<uint32_t, KIND_UNSIGNED, NoValue>(ctx, keys, nullptr, n_small, s);
+      if (rc == HPCS_OK) {
+        probe_check_kernel<<<ctx->sms * 4, 256, 0, s>>>(keys, it, n_small, bad);
+        if ((e = cudaGetLastError()) != cudaSuccess) rc = cuda_fail(e, "probe check");
+      }
     }
   }
   ctx->rank_mode = saved_mode;

@@ -1,5 +1,5 @@
-// LSD sort of a small array (keys only, at most SMALL_MAX_CTAS x SMALL_TILE keys) in one
-// cooperative launch.
+// LSD sort of a small array (keys, or keys with a 32-bit item each; at most SMALL_MAX_CTAS x
+// SMALL_TILE keys) in one cooperative launch.
 //
 // A sort of ~10^5 keys through the large-array kernels is a chain of launches (histogram, one
 // launch per digit pass, copy-back), each running on a handful of SMs with little to do, so its
@@ -12,8 +12,8 @@
 //   offsets  every CTA adds up all CTAs' totals (the global digit starts) and the totals of the
 //            CTAs before it (the bin-major, CTA-minor offsets of RadixSortLsdParallel.cs:49-94
 //            with one quantum per CTA);
-//   scatter  each key goes to its digit's start + its CTA's offset + its warp's offset + its
-//            rank; a grid barrier before the next pass reads the output.
+//   scatter  each key (and its item) goes to its digit's start + its CTA's offset + its warp's
+//            offset + its rank; a grid barrier before the next pass reads the output.
 // The launch is cooperative, so all G CTAs are resident together; the grid barrier's wait is
 // still bounded (spin_limit_ns) and records a timeout in the error word instead of hanging.
 // Keys written by other CTAs are read through L2 (ld.global.cg), never from a stale L1 line.
@@ -60,10 +60,12 @@ __device__ __forceinline__ U ld_cg_key(const U* p) {
   return U(__ldcg(reinterpret_cast<const unsigned long long*>(p)));
 }
 
-template <class U, int KIND, int MODE>
-__global__ void __launch_bounds__(SMALL_NT) small_sort_kernel(U* a, U* b, int n, uint32_t* counts, uint32_t* bar,
-                                                             uint32_t* err, uint64_t spin_limit_ns) {
+template <class U, int KIND, class V, int MODE>
+__global__ void __launch_bounds__(SMALL_NT) small_sort_kernel(U* a, U* b, uint32_t* va, uint32_t* vb, int n,
+                                                             uint32_t* counts, uint32_t* bar, uint32_t* err,
+                                                             uint64_t spin_limit_ns) {
   using KO = KeyOrder<U, KIND>;
+  constexpr bool PAIRS = !std::is_same<V, NoValue>::value;
   constexpr int P = int(sizeof(U));
   constexpr int NW = SMALL_NT / 32;
   __shared__ uint32_t s_cnt[NW][RADIX];  // per-warp digit counters, then per-(warp, digit) offsets
@@ -81,18 +83,22 @@ __global__ void __launch_bounds__(SMALL_NT) small_sort_kernel(U* a, U* b, int n,
   for (int p = 0; p < P; p++) {
     const U* src = (p & 1) ? b : a;
     U* dst = (p & 1) ? a : b;
+    const uint32_t* vsrc = (p & 1) ? vb : va;
+    uint32_t* vdst = (p & 1) ? va : vb;
     const int shift = 8 * p;
     for (int i = tid; i < NW * RADIX; i += SMALL_NT) (&s_cnt[0][0])[i] = 0u;
     if (MODE == RANK_PEER_MASK)
       for (int i = tid; i < NW * 2 * RADIX; i += SMALL_NT) s_msk[i] = 0u;
     __syncthreads();
     U key[SMALL_KPT];
+    uint32_t val[PAIRS ? SMALL_KPT : 1];
     uint32_t dg[SMALL_KPT], rank[SMALL_KPT];
     const int wbase = warp * 32 * SMALL_KPT;
 #pragma unroll
     for (int i = 0; i < SMALL_KPT; i++) {  // all loads issued before the first is used
       const int idx = wbase + i * 32 + lane;
       key[i] = idx < cnt_n ? ld_cg_key(src + lo + idx) : U(0);
+      if (PAIRS) val[PAIRS ? i : 0] = idx < cnt_n ? __ldcg(vsrc + lo + idx) : 0u;
     }
 #pragma unroll
     for (int i = 0; i < SMALL_KPT; i++) {
@@ -143,8 +149,12 @@ __global__ void __launch_bounds__(SMALL_NT) small_sort_kernel(U* a, U* b, int n,
       const int idx = wbase + i * 32 + lane;
       if (idx < cnt_n) {
         const uint32_t pos = s_base[dg[i]] + cnt_w[dg[i]] + rank[i];
-        if (pos < n32) dst[pos] = key[i];
-        else out_of_range = true;
+        if (pos < n32) {
+          dst[pos] = key[i];
+          if (PAIRS) vdst[pos] = val[PAIRS ? i : 0];
+        } else {
+          out_of_range = true;
+        }
       }
     }
     small_grid_barrier(bar, G, err, spin_limit_ns);  // the output is complete; counts may be reused

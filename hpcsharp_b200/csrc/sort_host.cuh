@@ -334,13 +334,16 @@ inline ChunkGeometry chunk_geometry(int64_t n, int tile, int max_ranges) {
 }
 
 // Enqueue a full LSD sort of n keys (and optional 4-byte items) in device memory.
-// A keys-only sort of at most SMALL_MAX_KEYS keys in one cooperative launch (small_sort.cuh),
+// A sort of at most SMALL_MAX_KEYS keys (and items) in one cooperative launch (small_sort.cuh),
 // with the context's ranking mode; scratch: B, the per-CTA digit totals and the barrier words.
-template <class U, int KIND>
-int enqueue_small_sort(hpcs_ctx* ctx, U* keys, int64_t n, cudaStream_t s) {
+template <class U, int KIND, class V>
+int enqueue_small_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t s) {
+  constexpr bool PAIRS = !std::is_same<V, NoValue>::value;
   const int G = int((n + SMALL_TILE - 1) / SMALL_TILE);
   int rc;
   if ((rc = ensure(ctx, ctx->keys_b, size_t(n) * sizeof(U))) != HPCS_OK) return rc;
+  if (PAIRS && (rc = ensure(ctx, ctx->vals_b, size_t(n) * 4)) != HPCS_OK) return rc;
+  uint32_t* vb = PAIRS ? static_cast<uint32_t*>(ctx->vals_b.ptr) : nullptr;
   if ((rc = ensure(ctx, ctx->status0, (size_t(G) * RADIX + 2) * 4)) != HPCS_OK) return rc;
   U* b = static_cast<U*>(ctx->keys_b.ptr);
   uint32_t* counts = static_cast<uint32_t*>(ctx->status0.ptr);
@@ -349,10 +352,10 @@ int enqueue_small_sort(hpcs_ctx* ctx, U* keys, int64_t n, cudaStream_t s) {
   int n32 = int(n);
   uint64_t spin = uint64_t(ctx->cfg.spin_limit_ns);
   HPCS_CUDA(cudaMemsetAsync(bar, 0, 2 * sizeof(uint32_t), s));
-  void* args[] = {&keys, &b, &n32, &counts, &bar, &err, &spin};
+  void* args[] = {&keys, &b, &vals, &vb, &n32, &counts, &bar, &err, &spin};
   const void* k = ctx->rank_mode == RANK_ORDERED_ATOMIC
-                      ? reinterpret_cast<const void*>(small_sort_kernel<U, KIND, RANK_ORDERED_ATOMIC>)
-                      : reinterpret_cast<const void*>(small_sort_kernel<U, KIND, RANK_PEER_MASK>);
+                      ? reinterpret_cast<const void*>(small_sort_kernel<U, KIND, V, RANK_ORDERED_ATOMIC>)
+                      : reinterpret_cast<const void*>(small_sort_kernel<U, KIND, V, RANK_PEER_MASK>);
   KernelTimer kt(ctx, s, HPCS_K_LOOKBACK);
   HPCS_CUDA(cudaLaunchCooperativeKernel(k, dim3(G), dim3(SMALL_NT), args, 0, s));
   return HPCS_OK;
@@ -366,12 +369,12 @@ int enqueue_sort(hpcs_ctx* ctx, U* keys, uint32_t* vals, int64_t n, cudaStream_t
   constexpr bool PAIRS = !std::is_same<V, NoValue>::value;
   if (n <= 1) return HPCS_OK;
   if (n > MAX_KEYS_PER_SORT) return fail(HPCS_ERR_RANGE, "n exceeds HPCS_MAX_KEYS");
-  // small keys-only sorts: one cooperative launch (not inside a stream capture, and not when a
-  // pass scheme is forced)
-  if (!PAIRS && n <= SMALL_MAX_KEYS && ctx->cfg.pass_scheme == HPCS_PASSES_AUTO) {
+  // small sorts: one cooperative launch (not inside a stream capture, and not when a pass
+  // scheme is forced)
+  if (n <= SMALL_MAX_KEYS && ctx->cfg.pass_scheme == HPCS_PASSES_AUTO) {
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     HPCS_CUDA(cudaStreamIsCapturing(s, &cap));
-    if (cap == cudaStreamCaptureStatusNone) return enqueue_small_sort<U, KIND>(ctx, keys, n, s);
+    if (cap == cudaStreamCaptureStatusNone) return enqueue_small_sort<U, KIND, V>(ctx, keys, vals, n, s);
   }
   if (ctx->cfg.pass_scheme == HPCS_PASSES_LOOKBACK && n > MAX_KEYS_LOOKBACK)
     return fail(HPCS_ERR_RANGE, "look-back passes take at most 2^30 - 1 keys (30-bit prefixes)");

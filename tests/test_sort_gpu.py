@@ -337,3 +337,21 @@ def test_small_sort_limits(orc, dt, n, rank_mode):
         assert_same_bits(got, want)
     finally:
         c.close()
+
+
+@pytest.mark.parametrize("rank_mode", [0, 1], ids=["ordered_atomic", "peer_mask"])
+@pytest.mark.parametrize("n", SMALL_SORT_SIZES)
+def test_small_pairs_sort_limits(orc, n, rank_mode):
+    """Key + index pairs of up to 128 Ki keys take the one-launch sort too: the permutation must
+    equal the oracle's stable pairs sort on both sides of the limit, in both ranking modes."""
+    keys = datagen.u64_zipf(n, seed=5 + n)
+    items = np.arange(n, dtype=np.uint32)
+    k2, i2 = keys.copy(), items.copy()
+    orc.sort_pairs(k2, i2)
+    c = native.Context(0, rank_mode=rank_mode)
+    try:
+        c.sort_pairs(keys, items)
+        np.testing.assert_array_equal(keys, k2)
+        np.testing.assert_array_equal(items, i2)
+    finally:
+        c.close()
