@@ -42,6 +42,9 @@ def test_status_strings_and_defaults():
     assert lib.hpcs_status_string(5) == b"HPCS_ERR_DEVICE_TIMEOUT"
     cfg = native.default_config()
     assert cfg.skip_trivial_passes == 1 and cfg.poison_tile == -1 and cfg.spin_limit_ns > 0
+    # the remaining settings default to the library's choices (0 = built-in value)
+    assert cfg.pass_scheme == 0 and cfg.staged_host_copies == 1
+    assert cfg.seg_grid_min_keys == 0 and cfg.seg_grid_tiles == 0 and list(cfg.reserved) == [0, 0, 0]
 
 
 def test_null_context_and_arrays_are_rejected_without_gpu():
