@@ -80,9 +80,11 @@ typedef struct hpcs_config {
   int64_t spin_limit_ns;       /* bound on every device-side wait (default 2e9) */
   int32_t poison_tile;         /* test hook: tile whose device wait times out (-1 = off) */
   int32_t pass_scheme;         /* digit passes: HPCS_PASSES_AUTO (0, default) picks by key
-                                  type and n; HPCS_PASSES_LOOKBACK (1): single-pass decoupled
-                                  look-back; HPCS_PASSES_CHUNKED (2): per-range counts from
-                                  the previous pass, no inter-CTA waiting */
+                                  type and n (up to 131072 keys: every pass in one cooperative
+                                  launch, outside stream capture); HPCS_PASSES_LOOKBACK (1):
+                                  single-pass decoupled look-back; HPCS_PASSES_CHUNKED (2):
+                                  per-range counts from the previous pass, no inter-CTA
+                                  waiting */
   int32_t staged_host_copies;  /* host-array calls on pageable memory (default 1): copy through
                                   the context's pinned buffers in chunks, several host threads
                                   copying while the DMA engine moves earlier chunks; 0: one
